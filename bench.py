@@ -1,0 +1,363 @@
+"""
+Benchmark of the sasmodels hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--config cylinder2d|sphere1d|magnetic]
+
+One step = one evaluation of the polydisperse, oriented cylinder 2D
+workload (256x256 (qx, qy) grid, 35x35x20x20 = 490000-point dispersity mesh,
+3.21e10 weighted q x mesh-point evaluations) through the driver kernels,
+inputs resident in HBM.  ``value`` is q x pd-point evaluations per second
+(all ranks).  ``e2e`` is the same metric through the public engine API with
+host buffers: each step builds a kernel for the q points (upload), evaluates
+I(q) from host ``details``/``values`` arrays and reads I(q) back.
+
+Multi-GPU (torchrun, one rank per GPU): every rank evaluates its own copy of
+the workload (independent detector images), no collective on the data path;
+timing is the max over ranks ("scaling": "weak").
+
+``--impl reference`` times the reference implementation of the same path on
+the host cores: the reference DLL kernel built from the reference's own C
+(oracle/_ref), q-sharded over all host threads, on a bounded sample of the
+same workload per step; rank 0 only.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = ("q×pd-point evals/s and fit param-sets/s at rel err ≤1e-5 vs FP64, "
+          "plain vs batched")
+UNIT = "evals/s"
+L2_FLUSH_BYTES = 256 << 20     # > 126 MB L2
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def workload(config):
+    from sasmodels_b200 import workloads
+    if config == "cylinder2d":
+        return workloads.cylinder_2d(), "cylinder 2D oriented FP64, 256x256 q, R(35) x L(35) x theta(20) x phi(20) mesh"
+    if config == "sphere1d":
+        return workloads.sphere_1d(), "sphere 1D FP64, 1000 log q, R gaussian pd 0.1 x 35"
+    if config == "magnetic":
+        return workloads.core_shell_sphere_magnetic(), "core_shell_sphere 2D magnetic FP64, 128x128 q, R(51 lognormal) x t(21)"
+    raise ValueError(config)
+
+
+def sample_workload(config):
+    """Bounded CPU sample of the same workload (full mesh, fewer q)."""
+    from sasmodels_b200 import workloads
+    if config == "cylinder2d":
+        return workloads.cylinder_2d_subgrid(32), "32x32 q block of the 256x256 grid, full 490000-point mesh"
+    if config == "sphere1d":
+        return workloads.sphere_1d(), "full workload"
+    if config == "magnetic":
+        name, (qx, qy), pars = workloads.core_shell_sphere_magnetic()
+        sub = np.arange(0, qx.size, 16)
+        return (name, [qx[sub], qy[sub]], pars), "every 16th q point (1024 q), full 1071-point mesh"
+    raise ValueError(config)
+
+
+def marshal(info, pars, q_vectors):
+    from sasmodels_b200.details import make_kernel_args
+    from sasmodels_b200.direct_model import get_mesh
+
+    class K:
+        pass
+    k = K()
+    k.info = info
+    k.dim = '2d' if len(q_vectors) == 2 else '1d'
+    k.dtype = np.dtype('d')
+    mesh = get_mesh(info, pars, dim=k.dim)
+    return make_kernel_args(k, mesh)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_%d.csv" % os.getpid())
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return None
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fid:
+            for line in fid:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                for name, flag in zip(names, parts[5:9]):
+                    if flag.lower() == "active":
+                        reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def dist_max(x):
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier():
+    import torch
+    import torch.distributed as dist
+    torch.cuda.synchronize()
+    if dist.is_available() and dist.is_initialized():
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def cpu_baseline(config, seconds_hint=None):
+    """Reference DLL (oracle/_ref) on a bounded sample with all host threads."""
+    from oracle import refdll
+    from sasmodels_b200 import load_model_info
+    (name, qv, pars), sample = sample_workload(config)
+    info = load_model_info(name)
+    details, values, magnetic = marshal(info, pars, qv)
+    dim = '2d' if len(qv) == 2 else '1d'
+    var = "Iq" if dim == '1d' else ("Imagnetic" if magnetic else "Iqxy")
+    nout = 2 if info.have_Fq and dim == '1d' else 1
+    if dim == '1d':
+        q = np.ascontiguousarray(qv[0])
+    else:
+        q = np.empty(2*len(qv[0]))
+        q[0::2], q[1::2] = qv
+    threads = host_threads()
+    evals = len(qv[0])*details.num_eval
+    refdll.run_threads(name, var, q[:2*min(threads, len(qv[0]))] if dim == '2d' else q[:threads],
+                       details.buffer, values, nout, threads)
+    t0 = time.perf_counter()
+    refdll.run_threads(name, var, q, details.buffer, values, nout, threads)
+    dt = time.perf_counter() - t0
+    return evals/dt, threads, sample, evals, dt
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    values = []
+    for step in range(args.warmup + args.steps):
+        v, threads, sample, evals, dt = cpu_baseline(args.config)
+        if step >= args.warmup:
+            values.append(v)
+    value = statistics.median(values)
+    (_, _, _), desc = workload(args.config)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3*evals/value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "sample": sample, "parallelism": "host threads, q-sharded"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, world, rank, local):
+    import torch
+    from sasmodels_b200 import load_model, peaks
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    (name, qv, pars), desc = workload(args.config)
+    model = load_model(name, device=dev)
+    kernel = model.make_kernel(qv)
+    details, values, magnetic = marshal(model.info, pars, qv)
+    variant = kernel.variant(magnetic)
+    nq = kernel.q_input.nq
+    n_mesh = details.num_eval
+    evals = nq*n_mesh
+    dev_d, dev_v = kernel.upload(details, values)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = kernel.stream
+    launches_per_step = 3   # mesh_prepare, iq_main, finalize
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            kernel.launch(variant, dev_d, dev_v, 0, n_mesh, 0.0, 0)
+    barrier()
+
+    times = []
+    with ClockSampler(local) as clocks:
+        barrier()
+        t_wall = time.perf_counter()
+        with torch.cuda.stream(stream):
+            for _ in range(args.steps):
+                flush.zero_()
+                start = torch.cuda.Event(enable_timing=True)
+                stop = torch.cuda.Event(enable_timing=True)
+                start.record(stream)
+                kernel.launch(variant, dev_d, dev_v, 0, n_mesh, 0.0, 0)
+                stop.record(stream)
+                times.append((start, stop))
+        barrier()
+        wall = time.perf_counter() - t_wall
+    step_s = [a.elapsed_time(b)*1e-3 for a, b in times]
+    t_total = dist_max(sum(step_s))
+    value = world*evals*args.steps/t_total
+    ms_per_step = 1e3*t_total/args.steps
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        qhost = [np.ascontiguousarray(v) for v in qv]
+        h2d = sum(v.nbytes for v in qhost) + details.buffer.nbytes + values.nbytes
+        d2h = kernel.result.nbytes
+        for _ in range(1):
+            k2 = model.make_kernel(qhost)
+            k2(details, values, 0.0, magnetic)
+            k2.release()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            k2 = model.make_kernel(qhost)
+            k2(details, values, 0.0, magnetic)
+            k2.release()
+        barrier()
+        te = dist_max(time.perf_counter() - t0)
+        e2e = {"value": world*evals*args.steps/te, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    line = None
+    if rank == 0:
+        fp64_peak = peaks.fp64_tflops()
+        flops_per_eval = FLOPS_PER_EVAL.get(args.config)
+        achieved = None
+        if flops_per_eval:
+            achieved = flops_per_eval*evals/(ms_per_step*1e-3)/1e12
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "evals_per_step": evals, "nq": nq,
+                       "mesh": n_mesh, "l2": "flushed (256 MB write) before each timed step",
+                       "parallelism": "replicas x%d (one workload per GPU)" % world},
+            "e2e": e2e,
+            "gpu_launches": launches_per_step*args.steps,
+            "wall_s": wall,
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak,
+                         "unit": "TFLOP/s",
+                         "frac": (achieved/fp64_peak) if achieved else None,
+                         "peak_source": "measured live: csrc/peaks.cu DFMA probe",
+                         "flops_per_eval": flops_per_eval,
+                         "traffic": TRAFFIC_PER_STEP.get(args.config)},
+        }
+        s = clocks.summary()
+        if s:
+            line["clocks"] = s
+        if world == 1 and not args.no_cpu:
+            v, threads, sample, _, _ = cpu_baseline(args.config)
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads,
+                                    "kind": "reference", "sample": sample}
+        print(json.dumps(line), flush=True)
+    return line
+
+
+#: FP64 flops issued per evaluation of each workload's dominant kernel,
+#: from the ncu instruction counters of iq_main (2*DFMA + DADD + DMUL per
+#: thread instruction) divided by the evaluations of the captured launch;
+#: see profiles/.
+FLOPS_PER_EVAL = {}
+#: dram read+write bytes of the dominant kernel per step (ncu), or None
+TRAFFIC_PER_STEP = {}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="cylinder2d",
+                    choices=["cylinder2d", "sphere1d", "magnetic"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args(argv)
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_b200(args, world, rank, local)
+    finally:
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,93 @@
+/*
+ * sasb200.h -- C-ABI of the B200 sasmodels engine.
+ *
+ * One shared library per model, libsasb200_<model>.so, exports the symbols
+ * below with <model> spliced into each name (SASB200_DECLARE_MODEL).  The
+ * libraries for sphere, cylinder, core_shell_sphere, ellipsoid and
+ * core_shell_cylinder are declared explicitly at the end of this file.
+ *
+ * Kernel entry points (one per kernel_iq.c instantiation)
+ * --------------------------------------------------------
+ *   sasb200_<model>_Iq         replaces <model>_Iq         (1D, CALL_FQ/CALL_IQ)
+ *   sasb200_<model>_Iqxy       replaces <model>_Iqxy       (2D, oriented or |q|)
+ *   sasb200_<model>_Imagnetic  replaces <model>_Imagnetic  (2D polarised)
+ *
+ * Reference interface replaced: the generated DLL kernel
+ *     void <model>_<variant>(int32_t nq, int32_t pd_start, int32_t pd_stop,
+ *         const ProblemDetails *details, const double *values,
+ *         const double *q, double *result, double cutoff,
+ *         int32_t radius_effective_mode)
+ * declared at sasmodels/kernel_iq.c:317-328, named by
+ * sasmodels/generate.py:635-642 and bound with ctypes at
+ * sasmodels/kerneldll.py:368-375 (called from DllKernel._call_kernel,
+ * sasmodels/kerneldll.py:449-475).
+ *
+ * The first nine arguments keep their meaning:
+ *   nq            number of q points (1D) or (qx, qy) pairs (2D)
+ *   pd_start/stop half-open range of the dispersity mesh to accumulate;
+ *                 pd_start == 0 starts a new sum, pd_start > 0 adds to the
+ *                 sums already in result (restartable mesh)
+ *   details       int32[4*max_pd + 4]  CallDetails buffer (details.py:43-180)
+ *   values        float64 packed parameter / dispersity vector
+ *                 (details.py:225-254)
+ *   q             float64[nq] (1D) or interleaved float64[2*nq] (2D)
+ *   result        float64[nout*nq + 4], nout = 2 for 1D models with Fq
+ *                 (F^2 at even, F at odd slots), else 1; the last four
+ *                 slots receive sum(w), sum(w V_form), sum(w V_shell),
+ *                 sum(w R_eff)
+ *   cutoff        mesh points with weight <= cutoff are skipped
+ *   radius_effective_mode   0 = skip R_eff, else the model's mode number
+ * All arrays are DEVICE pointers (any allocator).  Added arguments:
+ *   workspace, workspace_bytes  device scratch; sasb200_<model>_workspace_bytes
+ *                 gives the size for a whole mesh in one pass; a smaller
+ *                 workspace is used by processing the mesh in chunks
+ *   tile          iq_main tile code (splits<<16 | warps<<8 | lanes_per_q),
+ *                 0 = built-in choice; see sasb200_<model>_tile_code
+ *   stream        cudaStream_t (NULL = legacy default stream)
+ * Return: 0 on success; -1 bad argument, -2 workspace too small for one
+ * 128-point mesh segment, -3 CUDA launch error, -4 variant not available
+ * (e.g. Imagnetic for a model without sld parameters).  The calls are
+ * asynchronous on *stream*; sasb200_<model>_last_error() describes the last
+ * failure on the calling host thread.
+ */
+#ifndef SASB200_H
+#define SASB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SASB200_KERNEL_ARGS \
+    int32_t nq, int32_t pd_start, int32_t pd_stop, const int32_t *details, \
+    const double *values, const double *q, double *result, double cutoff, \
+    int32_t radius_effective_mode, void *workspace, uint64_t workspace_bytes, \
+    int32_t tile, void *stream
+
+#define SASB200_DECLARE_MODEL(M) \
+    int32_t sasb200_##M##_Iq(SASB200_KERNEL_ARGS); \
+    int32_t sasb200_##M##_Iqxy(SASB200_KERNEL_ARGS); \
+    int32_t sasb200_##M##_Imagnetic(SASB200_KERNEL_ARGS); \
+    /* bytes of workspace for variant 0=Iq 1=Iqxy 2=Imagnetic; no reference counterpart */ \
+    uint64_t sasb200_##M##_workspace_bytes(int32_t variant, int32_t nq, \
+                                           int32_t n_mesh, int32_t tile); \
+    /* number of instantiated tile shapes and the code of shape i (autotuner) */ \
+    int32_t sasb200_##M##_tile_count(void); \
+    int32_t sasb200_##M##_tile_code(int32_t i); \
+    /* tile code the library picks for (nq, n_mesh) when tile == 0 */ \
+    int32_t sasb200_##M##_default_tile(int32_t nq, int32_t n_mesh); \
+    /* message of the last failed call on this host thread ("" if none) */ \
+    const char *sasb200_##M##_last_error(void);
+
+SASB200_DECLARE_MODEL(sphere)
+SASB200_DECLARE_MODEL(cylinder)
+SASB200_DECLARE_MODEL(core_shell_sphere)
+SASB200_DECLARE_MODEL(ellipsoid)
+SASB200_DECLARE_MODEL(core_shell_cylinder)
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SASB200_H */

@@ -1,0 +1,116 @@
+"""
+ctypes binding of the per-model C-ABI (include/sasb200.h).
+
+Every symbol takes device pointers and a CUDA stream handle; nothing here
+allocates or copies.  A missing or unloadable library raises RuntimeError:
+there is no CPU fallback on the product path.
+"""
+
+import ctypes as ct
+import json
+import os
+
+LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
+
+VARIANTS = ("Iq", "Iqxy", "Imagnetic")
+VARIANT_ID = {name: k for k, name in enumerate(VARIANTS)}
+
+_KERNEL_ARGTYPES = [
+    ct.c_int32, ct.c_int32, ct.c_int32,      # nq, pd_start, pd_stop
+    ct.c_void_p, ct.c_void_p, ct.c_void_p,   # details, values, q
+    ct.c_void_p,                             # result
+    ct.c_double, ct.c_int32,                 # cutoff, radius_effective_mode
+    ct.c_void_p, ct.c_uint64,                # workspace, workspace_bytes
+    ct.c_int32, ct.c_void_p,                 # tile, stream
+]
+
+_LOADED = {}
+
+
+def library_path(name, lib_dir=None):
+    return os.path.join(lib_dir or LIB_DIR, "libsasb200_%s.so" % name)
+
+
+def metadata_path(name, lib_dir=None):
+    return os.path.join(lib_dir or LIB_DIR, "%s.json" % name)
+
+
+def available_models(lib_dir=None):
+    d = lib_dir or LIB_DIR
+    if not os.path.isdir(d):
+        return []
+    return sorted(f[len("libsasb200_"):-3] for f in os.listdir(d)
+                  if f.startswith("libsasb200_") and f.endswith(".so")
+                  and os.path.exists(os.path.join(d, f[len("libsasb200_"):-3] + ".json")))
+
+
+class ModelLib:
+    """The exported functions of one ``libsasb200_<name>.so``."""
+
+    def __init__(self, name, path=None):
+        self.name = name
+        self.path = path or library_path(name)
+        if not os.path.exists(self.path):
+            raise RuntimeError(
+                "B200 library for model %r not found at %s; run "
+                "`python -m sasmodels_b200.build %s`" % (name, self.path, name))
+        try:
+            self.lib = ct.CDLL(self.path)
+        except OSError as exc:
+            raise RuntimeError("cannot load %s: %s" % (self.path, exc)) from exc
+        self.kernels = {}
+        for variant in VARIANTS:
+            fn = getattr(self.lib, "sasb200_%s_%s" % (name, variant))
+            fn.argtypes = _KERNEL_ARGTYPES
+            fn.restype = ct.c_int32
+            self.kernels[variant] = fn
+        self._ws = self._fn("workspace_bytes", ct.c_uint64,
+                            [ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32])
+        self._err = self._fn("last_error", ct.c_char_p, [])
+        self._ntile = self._fn("tile_count", ct.c_int32, [])
+        self._tile = self._fn("tile_code", ct.c_int32, [ct.c_int32])
+        self._default_tile = self._fn("default_tile", ct.c_int32,
+                                      [ct.c_int32, ct.c_int32])
+
+    def _fn(self, suffix, restype, argtypes):
+        fn = getattr(self.lib, "sasb200_%s_%s" % (self.name, suffix))
+        fn.restype = restype
+        fn.argtypes = argtypes
+        return fn
+
+    def workspace_bytes(self, variant, nq, n_mesh, tile=0):
+        return int(self._ws(VARIANT_ID[variant], nq, n_mesh, tile))
+
+    def last_error(self):
+        msg = self._err()
+        return msg.decode() if msg else ""
+
+    def tile_shapes(self):
+        return [int(self._tile(i)) for i in range(int(self._ntile()))]
+
+    def default_tile(self, nq, n_mesh):
+        return int(self._default_tile(nq, n_mesh))
+
+    def call(self, variant, nq, pd_start, pd_stop, details, values, q, result,
+             cutoff, reff_mode, workspace, workspace_bytes, tile, stream):
+        status = self.kernels[variant](
+            nq, pd_start, pd_stop, details, values, q, result, cutoff,
+            reff_mode, workspace, workspace_bytes, tile, stream)
+        if status != 0:
+            raise RuntimeError("sasb200_%s_%s failed (%d): %s" % (
+                self.name, variant, status, self.last_error()))
+
+
+def load_library(name, lib_dir=None):
+    key = (name, lib_dir)
+    if key not in _LOADED:
+        _LOADED[key] = ModelLib(name, library_path(name, lib_dir))
+    return _LOADED[key]
+
+
+def load_metadata(name, lib_dir=None):
+    path = metadata_path(name, lib_dir)
+    if not os.path.exists(path):
+        raise RuntimeError("no B200 metadata for model %r at %s" % (name, path))
+    with open(path) as fid:
+        return json.load(fid)

@@ -1,0 +1,84 @@
+"""
+Model loading for the B200 backend, mirroring ``sasmodels/core.py``
+(``load_model`` 117-128, ``load_model_info`` 130-169, ``build_model``
+293-341).
+
+``load_model("cylinder")`` works from the prebuilt library and its JSON
+metadata alone.  ``build_model(info)`` also accepts a sasmodels
+``ModelInfo`` (and compiles the library if it is missing, which needs
+sasmodels' model sources and nvcc).  :func:`install` routes
+``sasmodels.core.build_model(..., platform="b200")`` here so existing
+callers (``direct_model``, ``bumps_model``, ``sasview_model``, product and
+mixture kernels) pick up the B200 engine without edits.
+"""
+
+import os
+
+from . import _abi
+from .kernel import B200Model
+from .modelinfo import ModelInfo
+
+PLATFORM = "b200"
+
+
+def list_models():
+    """Models with a built B200 library."""
+    return _abi.available_models()
+
+
+def load_model_info(name, lib_dir=None):
+    """Our :class:`ModelInfo` from the JSON written beside the library."""
+    return ModelInfo(_abi.load_metadata(name, lib_dir))
+
+
+def load_model(name, dtype="double", platform=PLATFORM, device=None):
+    """Engine for model *name* (``core.py:117-128``)."""
+    if platform != PLATFORM:
+        raise ValueError("sasmodels_b200 only provides platform %r" % PLATFORM)
+    return build_model(load_model_info(name), dtype=dtype, device=device)
+
+
+def build_model(model_info, dtype=None, platform=PLATFORM, device=None):
+    """Engine for *model_info*, ours or a sasmodels ModelInfo (``core.py:293-341``)."""
+    if platform not in (PLATFORM, None):
+        raise ValueError("sasmodels_b200 only provides platform %r" % PLATFORM)
+    info = model_info
+    if not isinstance(info, ModelInfo):
+        name = info.id
+        if name not in _abi.available_models():
+            from . import build
+            build.build_model(name)
+        info = load_model_info(name)
+    if dtype in ("single", "float32", "f", "float32c", "single!"):
+        from .fp32c import B200ModelF32c
+        return B200ModelF32c(info, device=device)
+    return B200Model(info, dtype="double", device=device)
+
+
+_ORIGINAL = {}
+
+
+def install():
+    """
+    Route ``sasmodels.core.build_model(info, dtype, platform="b200")`` (and
+    ``SAS_OPENCL=b200``) to this backend.  The reference package is left
+    untouched on disk; only the function object in its module is wrapped.
+    """
+    import sasmodels.core as sc
+    if "build_model" in _ORIGINAL:
+        return
+    original = sc.build_model
+    _ORIGINAL["build_model"] = original
+
+    def build_model_b200(model_info, dtype=None, platform="ocl"):
+        env = os.environ.get("SAS_OPENCL", "").lower()
+        if platform == PLATFORM or (platform == "ocl" and env == PLATFORM):
+            return build_model(model_info, dtype=dtype)
+        return original(model_info, dtype=dtype, platform=platform)
+    sc.build_model = build_model_b200
+
+
+def uninstall():
+    import sasmodels.core as sc
+    if "build_model" in _ORIGINAL:
+        sc.build_model = _ORIGINAL.pop("build_model")

@@ -1,0 +1,289 @@
+// C-ABI entry points around the driver templates of sas_driver.cuh.
+//
+// SASB200_EXPORT_MODEL(name, Model) defines, for one generated model binding,
+//
+//   int32_t  sasb200_<name>_Iq(...), _Iqxy(...), _Imagnetic(...)
+//   uint64_t sasb200_<name>_workspace_bytes(variant, nq, n_mesh, tile)
+//   int32_t  sasb200_<name>_tile_count(void), sasb200_<name>_tile_code(i)
+//   const char *sasb200_<name>_last_error(void)
+//
+// The three kernels take the arguments of the reference DLL symbols
+// <name>_Iq/_Iqxy/_Imagnetic (sasmodels/kernel_iq.c:317-328; ctypes argtypes
+// in sasmodels/kerneldll.py:368-375), with every array in device memory,
+// followed by a caller-owned device workspace, a tile code and a CUDA stream.
+// They return 0 on success and a negative code otherwise; no C++ exception
+// crosses the boundary.  See include/sasb200.h.
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <cuda_runtime.h>
+
+namespace sasb200 {
+
+enum Status {
+    OK = 0,
+    ERR_ARGUMENT = -1,
+    ERR_WORKSPACE = -2,
+    ERR_CUDA = -3,
+    ERR_UNSUPPORTED = -4,
+};
+
+struct Tile { int lq, warps, splits; };
+
+// (lq, warps) shapes instantiated for iq_main.
+constexpr int N_SHAPES = 6;
+__host__ inline Tile shape_at(int i)
+{
+    static const Tile shapes[N_SHAPES] = {
+        {32, 4, 1}, {32, 8, 1}, {8, 4, 1}, {8, 8, 1}, {1, 4, 1}, {1, 8, 1}};
+    return shapes[i];
+}
+
+// tile code = (splits << 16) | (warps << 8) | lq, or 0 for the built-in choice
+__host__ inline int32_t tile_encode(Tile t) { return (t.splits << 16) | (t.warps << 8) | t.lq; }
+__host__ inline Tile tile_decode(int32_t code)
+{
+    return Tile{code & 0xff, (code >> 8) & 0xff, (code >> 16) & 0xffff};
+}
+__host__ inline bool shape_ok(Tile t)
+{
+    for (int i = 0; i < N_SHAPES; ++i) {
+        const Tile s = shape_at(i);
+        if (s.lq == t.lq && s.warps == t.warps) return true;
+    }
+    return false;
+}
+
+__host__ inline int device_sms()
+{
+    static thread_local int cached_dev = -1, cached_sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return cached_sms;
+    if (dev != cached_dev) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess
+            && sms > 0) cached_sms = sms;
+        cached_dev = dev;
+    }
+    return cached_sms;
+}
+
+// Built-in tile choice: wide q tiles when there are many q points, mesh
+// lanes when there are few, then enough mesh splits to give every SM several
+// blocks.
+__host__ inline Tile choose_tile(int nq, int n_mesh)
+{
+    Tile t;
+    if (nq >= 4096) t = Tile{32, 4, 1};
+    else if (nq >= 256) t = Tile{8, 4, 1};
+    else t = Tile{1, 8, 1};
+    const long long qtiles = (nq + t.lq - 1)/t.lq;
+    const long long nseg = (n_mesh + SEG - 1)/SEG;
+    const long long want = (long long)device_sms()*16;
+    long long splits = qtiles > 0 ? (want + qtiles - 1)/qtiles : 1;
+    if (splits > nseg) splits = nseg;
+    if (splits > 4096) splits = 4096;
+    if (splits < 1) splits = 1;
+    t.splits = (int)splits;
+    return t;
+}
+
+__host__ inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+template <class M, int VAR>
+struct Workspace {
+    using L = Layout<M, VAR>;
+    size_t table, counts, norms, partial, total;
+    Workspace(int nq, long long chunk, int splits)
+    {
+        const long long nseg = (chunk + SEG - 1)/SEG;
+        table = align256((size_t)nseg*SEG*L::NF*sizeof(double));
+        counts = align256((size_t)nseg*sizeof(int));
+        norms = align256((size_t)nseg*4*sizeof(double));
+        partial = align256((size_t)(splits > 0 ? splits : 1)*L::NOUT*(size_t)nq*sizeof(double));
+        total = table + counts + norms + partial;
+    }
+};
+
+template <class M, int VAR, int LQ, int WARPS>
+__host__ void launch_main(dim3 grid, cudaStream_t st, int nq, const double *q,
+                          const double *values, const double *table,
+                          const int *counts, int nseg, double *partial)
+{
+    iq_main<M, VAR, LQ, WARPS><<<grid, 32*WARPS, 0, st>>>(
+        nq, q, values, table, counts, nseg, partial);
+}
+
+template <class M, int VAR>
+__host__ bool dispatch_main(Tile t, dim3 grid, cudaStream_t st, int nq, const double *q,
+                            const double *values, const double *table,
+                            const int *counts, int nseg, double *partial)
+{
+    switch (t.lq*100 + t.warps) {
+    case 3204: launch_main<M, VAR, 32, 4>(grid, st, nq, q, values, table, counts, nseg, partial); return true;
+    case 3208: launch_main<M, VAR, 32, 8>(grid, st, nq, q, values, table, counts, nseg, partial); return true;
+    case 804:  launch_main<M, VAR, 8, 4>(grid, st, nq, q, values, table, counts, nseg, partial); return true;
+    case 808:  launch_main<M, VAR, 8, 8>(grid, st, nq, q, values, table, counts, nseg, partial); return true;
+    case 104:  launch_main<M, VAR, 1, 4>(grid, st, nq, q, values, table, counts, nseg, partial); return true;
+    case 108:  launch_main<M, VAR, 1, 8>(grid, st, nq, q, values, table, counts, nseg, partial); return true;
+    default: return false;
+    }
+}
+
+// Error text of the last failing call on this host thread.
+inline char *error_buffer()
+{
+    static thread_local char buf[256] = "";
+    return buf;
+}
+
+__host__ inline int32_t fail(int32_t code, const char *msg)
+{
+    std::snprintf(error_buffer(), 256, "%s", msg);
+    return code;
+}
+
+template <class M, int VAR>
+__host__ uint64_t workspace_bytes(int32_t nq, int32_t n_mesh, int32_t tile_code)
+{
+    if (nq < 0 || n_mesh < 0) return 0;
+    Tile t = tile_code ? tile_decode(tile_code) : choose_tile(nq, n_mesh);
+    const long long chunk = n_mesh < (1 << 20) ? n_mesh : (1 << 20);
+    return Workspace<M, VAR>(nq, chunk, t.splits).total;
+}
+
+// One kernel call: mesh [pd_start, pd_stop) is processed in chunks that fit
+// the workspace; the first chunk overwrites result unless pd_start > 0
+// (restartable mesh, kernel_iq.c:381-423), later chunks add to it.
+template <class M, int VAR>
+__host__ int32_t run(int32_t nq, int32_t pd_start, int32_t pd_stop,
+                     const int32_t *details, const double *values, const double *q,
+                     double *result, double cutoff, int32_t reff_mode,
+                     void *workspace, uint64_t workspace_bytes, int32_t tile_code,
+                     void *stream)
+{
+    using L = Layout<M, VAR>;
+    error_buffer()[0] = 0;
+    if constexpr (VAR == VAR_IMAGNETIC && M::NMAG == 0) {
+        return fail(ERR_UNSUPPORTED, "model has no magnetic parameters");
+    } else {
+    if (nq < 0 || pd_start < 0 || pd_stop < pd_start)
+        return fail(ERR_ARGUMENT, "need nq >= 0 and 0 <= pd_start <= pd_stop");
+    if (!details || !values || !result || (nq > 0 && !q))
+        return fail(ERR_ARGUMENT, "null array pointer");
+    const int n_mesh = pd_stop - pd_start;
+    Tile t = tile_code ? tile_decode(tile_code) : choose_tile(nq, n_mesh);
+    if (!shape_ok(t) || t.splits < 1)
+        return fail(ERR_ARGUMENT, "unknown tile code");
+    // largest chunk of whole segments whose workspace fits
+    const long long nseg_all = n_mesh > 0 ? (n_mesh + SEG - 1)/SEG : 1;
+    long long lo = 0, hi = nseg_all;
+    while (lo < hi) {
+        const long long mid = (lo + hi + 1)/2;
+        if (Workspace<M, VAR>(nq, mid*SEG, t.splits).total <= workspace_bytes) lo = mid;
+        else hi = mid - 1;
+    }
+    if (lo == 0 || !workspace)
+        return fail(ERR_WORKSPACE, "workspace too small for one mesh segment");
+    const long long chunk = lo == nseg_all ? (n_mesh > 0 ? n_mesh : 1) : lo*SEG;
+    const Workspace<M, VAR> ws(nq, chunk, t.splits);
+    char *base = static_cast<char *>(workspace);
+    double *table = reinterpret_cast<double *>(base);
+    int *counts = reinterpret_cast<int *>(base + ws.table);
+    double *norms = reinterpret_cast<double *>(base + ws.table + ws.counts);
+    double *partial = reinterpret_cast<double *>(base + ws.table + ws.counts + ws.norms);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int nout_nq = L::NOUT*nq;
+
+    long long start = pd_start;
+    do {
+        const int n = (int)((pd_stop - start) < chunk ? (pd_stop - start) : chunk);
+        const int nseg = (n + SEG - 1)/SEG;
+        int splits = t.splits < nseg ? t.splits : nseg;
+        if (nseg > 0) {
+            mesh_prepare<M, VAR><<<nseg, SEG, 0, st>>>(
+                (int)start, n, details, values, cutoff, reff_mode, table, counts, norms);
+        }
+        if (nq > 0 && nseg > 0) {
+            dim3 grid((nq + t.lq - 1)/t.lq, splits);
+            if (!dispatch_main<M, VAR>(t, grid, st, nq, q, values, table, counts, nseg, partial))
+                return fail(ERR_ARGUMENT, "unknown tile shape");
+        }
+        if (nseg == 0) splits = 0;
+        const int fblocks = (nout_nq + 255)/256 + 1;
+        finalize<0><<<fblocks, 256, 0, st>>>(nout_nq, splits, partial, nseg, norms, result,
+                                          start > 0 ? 1 : 0);
+        const cudaError_t err = cudaGetLastError();
+        if (err != cudaSuccess) {
+            std::snprintf(error_buffer(), 256, "kernel launch: %s", cudaGetErrorString(err));
+            return ERR_CUDA;
+        }
+        start += n;
+    } while (start < pd_stop);
+    return OK;
+    }
+}
+
+}  // namespace sasb200
+
+#define SASB200_STR2(x) #x
+#define SASB200_STR(x) SASB200_STR2(x)
+
+#define SASB200_EXPORT_MODEL(NAME, MODEL)                                               \
+extern "C" int32_t sasb200_##NAME##_Iq(                                                 \
+    int32_t nq, int32_t pd_start, int32_t pd_stop, const int32_t *details,              \
+    const double *values, const double *q, double *result, double cutoff,               \
+    int32_t radius_effective_mode, void *workspace, uint64_t workspace_bytes,           \
+    int32_t tile, void *stream)                                                         \
+{                                                                                       \
+    return sasb200::run<MODEL, sasb200::VAR_IQ>(nq, pd_start, pd_stop, details, values, \
+        q, result, cutoff, radius_effective_mode, workspace, workspace_bytes, tile,     \
+        stream);                                                                        \
+}                                                                                       \
+extern "C" int32_t sasb200_##NAME##_Iqxy(                                               \
+    int32_t nq, int32_t pd_start, int32_t pd_stop, const int32_t *details,              \
+    const double *values, const double *q, double *result, double cutoff,               \
+    int32_t radius_effective_mode, void *workspace, uint64_t workspace_bytes,           \
+    int32_t tile, void *stream)                                                         \
+{                                                                                       \
+    return sasb200::run<MODEL, sasb200::VAR_IQXY>(nq, pd_start, pd_stop, details,       \
+        values, q, result, cutoff, radius_effective_mode, workspace, workspace_bytes,   \
+        tile, stream);                                                                  \
+}                                                                                       \
+extern "C" int32_t sasb200_##NAME##_Imagnetic(                                          \
+    int32_t nq, int32_t pd_start, int32_t pd_stop, const int32_t *details,              \
+    const double *values, const double *q, double *result, double cutoff,               \
+    int32_t radius_effective_mode, void *workspace, uint64_t workspace_bytes,           \
+    int32_t tile, void *stream)                                                         \
+{                                                                                       \
+    return sasb200::run<MODEL, sasb200::VAR_IMAGNETIC>(nq, pd_start, pd_stop, details,  \
+        values, q, result, cutoff, radius_effective_mode, workspace, workspace_bytes,   \
+        tile, stream);                                                                  \
+}                                                                                       \
+extern "C" uint64_t sasb200_##NAME##_workspace_bytes(                                   \
+    int32_t variant, int32_t nq, int32_t n_mesh, int32_t tile)                          \
+{                                                                                       \
+    switch (variant) {                                                                  \
+    case 0: return sasb200::workspace_bytes<MODEL, sasb200::VAR_IQ>(nq, n_mesh, tile);  \
+    case 1: return sasb200::workspace_bytes<MODEL, sasb200::VAR_IQXY>(nq, n_mesh, tile);\
+    case 2: return sasb200::workspace_bytes<MODEL, sasb200::VAR_IMAGNETIC>(nq, n_mesh,  \
+                                                                           tile);       \
+    default: return 0;                                                                  \
+    }                                                                                   \
+}                                                                                       \
+extern "C" int32_t sasb200_##NAME##_tile_count(void) { return sasb200::N_SHAPES; }      \
+extern "C" int32_t sasb200_##NAME##_tile_code(int32_t i)                                \
+{                                                                                       \
+    if (i < 0 || i >= sasb200::N_SHAPES) return 0;                                      \
+    return sasb200::tile_encode(sasb200::shape_at(i));                                  \
+}                                                                                       \
+extern "C" int32_t sasb200_##NAME##_default_tile(int32_t nq, int32_t n_mesh)            \
+{                                                                                       \
+    return sasb200::tile_encode(sasb200::choose_tile(nq, n_mesh));                       \
+}                                                                                       \
+extern "C" const char *sasb200_##NAME##_last_error(void)                                \
+{                                                                                       \
+    return sasb200::error_buffer();                                                     \
+}

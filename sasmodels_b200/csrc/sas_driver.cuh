@@ -1,0 +1,512 @@
+// B200 polydispersity / orientation / magnetism driver.
+//
+// Replaces the generic kernel driver of the reference (sasmodels/kernel_iq.c)
+// for one model M (a SasModel binding struct emitted by the generator).  The
+// computation is the same weighted sum,
+//
+//     result[q]      = sum_{mesh points k, weight_k > cutoff, VALID}  w_k F^2(q; p_k)
+//     result[tail+0] = sum_k w_k,   tail+1: sum_k w_k V_form,
+//     tail+2: sum_k w_k V_shell,    tail+3: sum_k w_k R_eff
+//
+// but organised for the GPU in three launches instead of one thread per q
+// walking the whole mesh:
+//
+//   1. mesh_prepare  one thread per mesh point decodes the mixed-radix index,
+//                    forms the weight product, applies VALID, the jitter
+//                    projection and the cutoff, accumulates the volume norms,
+//                    builds the per-point rotation, and writes the surviving
+//                    points compacted into 128-point segments of an
+//                    array-of-structs table [weight, p[0..NPARS), rotation].
+//   2. iq_main       q tiles map to thread blocks.  Within a warp LQ lanes take
+//                    LQ neighbouring q and the 32/LQ lane groups take different
+//                    mesh points; the WARPS warps of a block interleave over
+//                    the segment, which is staged in shared memory.  FP64
+//                    partial sums are reduced with warp shuffles, then across
+//                    warps through shared memory, then written per mesh split.
+//   3. finalize      sums the mesh splits in a fixed order and the segment
+//                    norms in a fixed tree, and writes (or, for a restarted
+//                    call, adds to) the result vector.
+//
+// Every reduction has a fixed order that depends only on the tile shape, so a
+// call is bitwise reproducible.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sasb200 {
+
+enum Variant { VAR_IQ = 0, VAR_IQXY = 1, VAR_IMAGNETIC = 2 };
+enum XYMode { XY_1D = 0, XY_QA = 1, XY_QAC = 2, XY_QABC = 3, XY_QXY = 4 };
+
+// Mesh points per segment (and threads per mesh_prepare block).
+constexpr int SEG = 128;
+constexpr unsigned FULL_MASK = 0xffffffffu;
+
+// Mixed-radix mesh descriptor, the int32 CallDetails buffer
+// (kernel_iq.c:47-58, details.py:43-113) for a model with MPD pd slots.
+template <int MPD>
+struct DetailsView {
+    const int32_t *buf;
+    __device__ int pd_par(int d) const { return buf[d]; }
+    __device__ int pd_length(int d) const { return buf[MPD + d]; }
+    __device__ int pd_offset(int d) const { return buf[2*MPD + d]; }
+    __device__ int pd_stride(int d) const { return buf[3*MPD + d]; }
+    __device__ int num_eval() const { return buf[4*MPD]; }
+    __device__ int num_weights() const { return buf[4*MPD + 1]; }
+    __device__ int theta_par() const { return buf[4*MPD + 3]; }
+};
+
+// Per-variant table layout.
+template <class M, int VAR>
+struct Layout {
+    static constexpr int XY = (VAR == VAR_IQ) ? XY_1D : M::XY_MODE;
+    static constexpr int NROT = (XY == XY_QAC) ? 2 : (XY == XY_QABC) ? 6 : 0;
+    static constexpr int NP = M::NPARS > 0 ? M::NPARS : 1;
+    static constexpr int NF = ((1 + M::NPARS + NROT) + 1) & ~1;   // 16-byte rows
+    static constexpr bool FQ1D = (VAR == VAR_IQ) && M::HAVE_FQ;
+    static constexpr int NOUT = FQ1D ? 2 : 1;
+};
+
+// ------------------------------------------------------------- rotations ---
+// View (theta, phi[, psi]) followed by jitter (dtheta, dphi[, dpsi]) as the
+// reverse rotation from detector (qx, qy) to particle (qa, qb, qc).  Same
+// matrix products as kernel_iq.c:197-226 and 257-299.
+
+__device__ __forceinline__ void rotation_ac(double theta, double phi,
+                                            double dtheta, double dphi,
+                                            double *R)
+{
+    double st, ct, sp, cp;
+    sincos(theta*M_PI_180, &st, &ct);
+    sincos(phi*M_PI_180, &sp, &cp);
+    const double V11 = cp*ct, V12 = sp*ct;
+    const double V21 = -sp, V22 = cp;
+    const double V31 = st*cp, V32 = sp*st;
+    sincos(dtheta*M_PI_180, &st, &ct);
+    sincos(dphi*M_PI_180, &sp, &cp);
+    const double J31 = st, J32 = -sp*ct, J33 = cp*ct;
+    R[0] = J31*V11 + J32*V21 + J33*V31;
+    R[1] = J31*V12 + J32*V22 + J33*V32;
+}
+
+__device__ __forceinline__ void rotation_abc(double theta, double phi, double psi,
+                                             double dtheta, double dphi, double dpsi,
+                                             double *R)
+{
+    double st, ct, sp, cp, ss, cs;
+    sincos(theta*M_PI_180, &st, &ct);
+    sincos(phi*M_PI_180, &sp, &cp);
+    sincos(psi*M_PI_180, &ss, &cs);
+    const double V11 = -sp*ss + cp*cs*ct;
+    const double V12 = sp*cs*ct + ss*cp;
+    const double V21 = -sp*cs - ss*cp*ct;
+    const double V22 = -sp*ss*ct + cp*cs;
+    const double V31 = st*cp;
+    const double V32 = sp*st;
+    sincos(dtheta*M_PI_180, &st, &ct);
+    sincos(dphi*M_PI_180, &sp, &cp);
+    sincos(dpsi*M_PI_180, &ss, &cs);
+    const double J11 = cs*ct;
+    const double J12 = sp*st*cs + ss*cp;
+    const double J13 = sp*ss - st*cp*cs;
+    const double J21 = -ss*ct;
+    const double J22 = -sp*ss*st + cp*cs;
+    const double J23 = sp*cs + ss*st*cp;
+    const double J31 = st;
+    const double J32 = -sp*ct;
+    const double J33 = cp*ct;
+    R[0] = J11*V11 + J12*V21 + J13*V31;   // R11
+    R[1] = J11*V12 + J12*V22 + J13*V32;   // R12
+    R[2] = J21*V11 + J22*V21 + J23*V31;   // R21
+    R[3] = J21*V12 + J22*V22 + J23*V32;   // R22
+    R[4] = J31*V11 + J32*V21 + J33*V31;   // R31
+    R[5] = J31*V12 + J32*V22 + J33*V32;   // R32
+}
+
+// ------------------------------------------------------------- magnetism ---
+// Spin-resolved cross sections (kernel_iq.c:84-175).  Channel order:
+// 0 dd, 1 du.real, 2 ud.real, 3 uu, 4 du.imag, 5 ud.imag.
+
+struct SpinSetup {
+    double w[6];
+    double cos_mtheta, sin_mtheta, cos_mphi, sin_mphi;
+};
+
+__device__ __forceinline__ double clip01(double x)
+{
+    return x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x);
+}
+
+// Polarisation-efficiency weights of the six channels.  The normalisation
+// makes spin-resolved measurements add up to the (half-)polarised cross
+// section: it is the out-going efficiency, or 1 - it when the analyser
+// flips the spin (kernel_iq.c:84-124).
+__device__ __forceinline__ void spin_setup(const double *values, int npars, SpinSetup &s)
+{
+    const double in_spin = clip01(values[npars + 2]);
+    const double out_spin = clip01(values[npars + 3]);
+    const double norm = out_spin < 0.5 ? 1.0 - out_spin : out_spin;
+    s.w[0] = (1.0 - in_spin)*(1.0 - out_spin)/norm;
+    s.w[1] = (1.0 - in_spin)*out_spin/norm;
+    s.w[2] = in_spin*(1.0 - out_spin)/norm;
+    s.w[3] = in_spin*out_spin/norm;
+    s.w[4] = s.w[1];
+    s.w[5] = s.w[2];
+    sincos(values[npars + 4]*M_PI_180, &s.sin_mtheta, &s.cos_mtheta);
+    sincos(values[npars + 5]*M_PI_180, &s.sin_mphi, &s.cos_mphi);
+}
+
+// Effective sld of one magnetic sld in the five distinct channels
+// {dd, du.real (= ud.real), uu, du.imag, ud.imag} at detector point (qx, qy).
+// M_perp is the magnetisation with its component along q removed; P is the
+// polarisation axis and (perpy, perpz) span the plane normal to it.
+__device__ __forceinline__ void magnetic_slds(const SpinSetup &s, double qx, double qy,
+                                              double sld, double mx, double my, double mz,
+                                              double *eff5)
+{
+    const double qn = sqrt(qx*qx + qy*qy);
+    double qhat[3], M[3], P[3], perpy[3], perpz[3], Mperp[3];
+    SET_VEC(qhat, qx/qn, qy/qn, 0);
+    SET_VEC(M, mx, my, mz);
+    SET_VEC(P, s.sin_mtheta*s.cos_mphi, s.sin_mtheta*s.sin_mphi, s.cos_mtheta);
+    SET_VEC(perpy, -s.sin_mphi, s.cos_mphi, 0);
+    SET_VEC(perpz, -s.cos_mtheta*s.cos_mphi, -s.cos_mtheta*s.sin_mphi, s.sin_mtheta);
+    ORTH_VEC(Mperp, M, qhat);
+    const double pm = SCALAR_VEC(P, Mperp);
+    const double ym = SCALAR_VEC(perpy, Mperp);
+    const double zm = SCALAR_VEC(perpz, Mperp);
+    eff5[0] = sld - pm;     // dd
+    eff5[1] = ym;           // du.real and ud.real
+    eff5[2] = sld + pm;     // uu
+    eff5[3] = -zm;          // du.imag
+    eff5[4] = +zm;          // ud.imag
+}
+
+// ------------------------------------------------------ model evaluation ---
+
+template <class M, int XY>
+__device__ __forceinline__ double eval_2d(double qx, double qy, double qk,
+                                          const double *rot, const double *v)
+{
+    if constexpr (XY == XY_QA) {
+        return M::iq(qk, v);
+    } else if constexpr (XY == XY_QAC) {
+        // qab^2 = |q|^2 - qc^2 (kernel_iq.c:230-242)
+        const double qc = rot[0]*qx + rot[1]*qy;
+        const double qab_sq = -qc*qc + qx*qx + qy*qy;
+        const double qab = qab_sq > 0.0 ? sqrt(qab_sq) : 0.0;
+        return M::iqac(qab, qc, v);
+    } else if constexpr (XY == XY_QABC) {
+        const double qa = rot[0]*qx + rot[1]*qy;
+        const double qb = rot[2]*qx + rot[3]*qy;
+        const double qc = rot[4]*qx + rot[5]*qy;
+        return M::iqabc(qa, qb, qc, v);
+    } else {
+        return M::iqxy(qx, qy, v);
+    }
+}
+
+// ----------------------------------------------------------- mesh_prepare ---
+
+template <class M, int VAR>
+__global__ void __launch_bounds__(SEG)
+mesh_prepare(int pd_start, int n_mesh, const int32_t *__restrict__ details,
+             const double *__restrict__ values, double cutoff, int reff_mode,
+             double *__restrict__ table, int *__restrict__ seg_count,
+             double *__restrict__ seg_norm)
+{
+    using L = Layout<M, VAR>;
+    constexpr int MPD = M::MAX_PD;
+    constexpr int NF = L::NF;
+    const DetailsView<MPD> det{details};
+    const int t = threadIdx.x;
+    const int local = blockIdx.x*SEG + t;
+    const int step = pd_start + local;
+
+    bool keep = false;
+    double v[L::NP];
+    double weight = 0.0, form = 0.0, shell = 0.0, reff = 0.0;
+    double rot[L::NROT > 0 ? L::NROT : 1];
+
+    if (local < n_mesh) {
+        #pragma unroll
+        for (int k = 0; k < M::NPARS; ++k) v[k] = values[2 + k];
+        // Oriented 2D kernels start from zero jitter (kernel_iq.c:614-616, 559).
+        if constexpr (L::XY == XY_QAC || L::XY == XY_QABC) {
+            if (M::THETA_PAR >= 0) {
+                v[M::THETA_PAR] = 0.0;
+                v[M::THETA_PAR + 1] = 0.0;
+                if (L::XY == XY_QABC) v[M::THETA_PAR + 2] = 0.0;
+            }
+        }
+        const double *pd_value = values + M::NVALUES;
+        const double *pd_weight = pd_value + det.num_weights();
+        // weight_d = w_d[i_d] * weight_{d+1}, outermost level first
+        // (kernel_iq.c:642-664)
+        double w = 1.0;
+        #pragma unroll
+        for (int d = MPD - 1; d >= 0; --d) {
+            // lengths and strides were validated on the host; the max() only
+            // keeps a malformed buffer from dividing by zero
+            const int n = max(det.pd_length(d), 1);
+            const int i = (step/max(det.pd_stride(d), 1)) % n;
+            const int off = det.pd_offset(d) + i;
+            const int p = det.pd_par(d);
+            const double pv = pd_value[off];
+            #pragma unroll
+            for (int k = 0; k < M::NPARS; ++k) if (k == p) v[k] = pv;
+            w = pd_weight[off]*w;
+        }
+        if (M::valid(v)) {
+            if constexpr (L::XY == XY_QAC || L::XY == XY_QABC) {
+                const double dtheta = v[M::THETA_PAR];
+                weight = fabs(cos(dtheta*M_PI_180))*w;     // equirectangular
+            } else {
+                weight = w;
+            }
+            if constexpr (L::XY == XY_QXY) {
+                // models taking the angles directly see the view angles
+                if (M::HAVE_THETA) {
+                    v[M::THETA_PAR] = values[M::THETA_PAR + 2];
+                    v[M::THETA_PAR + 1] = values[M::THETA_PAR + 3];
+                    if (M::HAVE_PSI) v[M::THETA_PAR + 2] = values[M::THETA_PAR + 4];
+                }
+            }
+            if (weight > cutoff) {
+                keep = true;
+                M::volume(v, form, shell);
+                if (reff_mode != 0) reff = M::reff(reff_mode, v);
+                if constexpr (L::XY == XY_QAC) {
+                    rotation_ac(values[M::THETA_PAR + 2], values[M::THETA_PAR + 3],
+                                v[M::THETA_PAR], v[M::THETA_PAR + 1], rot);
+                } else if constexpr (L::XY == XY_QABC) {
+                    rotation_abc(values[M::THETA_PAR + 2], values[M::THETA_PAR + 3],
+                                 values[M::THETA_PAR + 4], v[M::THETA_PAR],
+                                 v[M::THETA_PAR + 1], v[M::THETA_PAR + 2], rot);
+                }
+            }
+        }
+    }
+
+    // Block-local stable compaction: ballot within warps, prefix over warps.
+    __shared__ int warp_base[SEG/32];
+    __shared__ double norm_red[4][SEG];
+    const int lane = t & 31, warp = t >> 5;
+    const unsigned ballot = __ballot_sync(FULL_MASK, keep);
+    if (lane == 0) warp_base[warp] = __popc(ballot);
+    norm_red[0][t] = keep ? weight : 0.0;
+    norm_red[1][t] = keep ? weight*form : 0.0;
+    norm_red[2][t] = keep ? weight*shell : 0.0;
+    norm_red[3][t] = keep ? weight*reff : 0.0;
+    __syncthreads();
+    int base = 0, total = 0;
+    #pragma unroll
+    for (int k = 0; k < SEG/32; ++k) {
+        if (k < warp) base += warp_base[k];
+        total += warp_base[k];
+    }
+    if (keep) {
+        const int pos = base + __popc(ballot & ((1u << lane) - 1u));
+        double *row = table + ((size_t)blockIdx.x*SEG + pos)*NF;
+        row[0] = weight;
+        #pragma unroll
+        for (int k = 0; k < M::NPARS; ++k) row[1 + k] = v[k];
+        #pragma unroll
+        for (int r = 0; r < L::NROT; ++r) row[1 + M::NPARS + r] = rot[r];
+    }
+    // fixed-order tree for the four norm sums
+    #pragma unroll
+    for (int s = SEG/2; s > 0; s >>= 1) {
+        __syncthreads();
+        if (t < s) {
+            #pragma unroll
+            for (int k = 0; k < 4; ++k) norm_red[k][t] += norm_red[k][t + s];
+        }
+    }
+    if (t == 0) {
+        seg_count[blockIdx.x] = total;
+        #pragma unroll
+        for (int k = 0; k < 4; ++k) seg_norm[4*blockIdx.x + k] = norm_red[k][0];
+    }
+}
+
+// ---------------------------------------------------------------- iq_main ---
+
+template <class M, int VAR, int LQ, int WARPS>
+__global__ void __launch_bounds__(32*WARPS)
+iq_main(int nq, const double *__restrict__ q, const double *__restrict__ values,
+        const double *__restrict__ table, const int *__restrict__ seg_count,
+        int nseg, double *__restrict__ partial)
+{
+    using L = Layout<M, VAR>;
+    constexpr int NF = L::NF;
+    constexpr int LM = 32/LQ;
+    constexpr int XY = L::XY;
+    constexpr bool MAG = (VAR == VAR_IMAGNETIC) && (M::NMAG > 0);
+    constexpr int NMAGS = M::NMAG > 0 ? M::NMAG : 1;
+
+    __shared__ __align__(16) double stage[SEG*NF];
+    __shared__ double red[WARPS][LQ][L::NOUT];
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int qi = lane % LQ;
+    const int ml = lane / LQ;
+    const int q_index = blockIdx.x*LQ + qi;
+    const bool q_ok = q_index < nq;
+    const int qload = q_ok ? q_index : 0;
+
+    double qk = 0.0, qx = 0.0, qy = 0.0;
+    if constexpr (XY == XY_1D) {
+        qk = q[qload];
+    } else {
+        qx = q[2*qload];
+        qy = q[2*qload + 1];
+        qk = sqrt(qx*qx + qy*qy);
+    }
+
+    // magnetism: per-q effective slds, hoisted out of the mesh loop
+    double eff[5][NMAGS];
+    double chan_w[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    bool mag_on = false;
+    if constexpr (MAG) {
+        SpinSetup s;
+        spin_setup(values, M::NPARS, s);
+        mag_on = (qx*qx + qy*qy) > 1.e-16;
+        // channels whose weight is significant (kernel_iq.c:759-761); the two
+        // real spin-flip channels see identical slds and share one evaluation
+        chan_w[0] = s.w[0] > 1.e-8 ? s.w[0] : 0.0;
+        chan_w[1] = (s.w[1] > 1.e-8 ? s.w[1] : 0.0) + (s.w[2] > 1.e-8 ? s.w[2] : 0.0);
+        chan_w[2] = s.w[3] > 1.e-8 ? s.w[3] : 0.0;
+        chan_w[3] = s.w[4] > 1.e-8 ? s.w[4] : 0.0;
+        chan_w[4] = s.w[5] > 1.e-8 ? s.w[5] : 0.0;
+        #pragma unroll
+        for (int sk = 0; sk < M::NMAG; ++sk) {
+            const int idx = M::mag_par(sk);
+            const double *m = values + M::NPARS + 6 + 3*sk;
+            double e5[5];
+            if (mag_on) magnetic_slds(s, qx, qy, values[idx + 2], m[0], m[1], m[2], e5);
+            else { e5[0] = e5[1] = e5[2] = e5[3] = e5[4] = 0.0; }
+            #pragma unroll
+            for (int c = 0; c < 5; ++c) eff[c][sk] = e5[c];
+        }
+    }
+
+    const int s0 = (int)(((long long)blockIdx.y*nseg)/gridDim.y);
+    const int s1 = (int)(((long long)(blockIdx.y + 1)*nseg)/gridDim.y);
+    double acc2 = 0.0, acc1 = 0.0;
+
+    for (int sgi = s0; sgi < s1; ++sgi) {
+        const int cnt = seg_count[sgi];
+        __syncthreads();
+        const double *src = table + (size_t)sgi*SEG*NF;
+        for (int i = threadIdx.x; i < cnt*NF; i += 32*WARPS) stage[i] = src[i];
+        __syncthreads();
+        for (int j = warp*LM + ml; j < cnt; j += WARPS*LM) {
+            const double *row = stage + j*NF;
+            const double w = row[0];
+            double v[L::NP];
+            #pragma unroll
+            for (int k = 0; k < M::NPARS; ++k) v[k] = row[1 + k];
+            const double *rot = row + 1 + M::NPARS;
+            if constexpr (XY == XY_1D) {
+                if constexpr (L::FQ1D) {
+                    double F1, F2;
+                    M::fq(qk, F1, F2, v);
+                    acc2 += w*F2;
+                    acc1 += w*F1;
+                } else {
+                    acc2 += w*M::iq(qk, v);
+                }
+            } else if constexpr (MAG) {
+                double F2 = 0.0;
+                if (mag_on) {
+                    #pragma unroll
+                    for (int c = 0; c < 5; ++c) {
+                        if (chan_w[c] > 0.0) {
+                            #pragma unroll
+                            for (int sk = 0; sk < M::NMAG; ++sk) v[M::mag_par(sk)] = eff[c][sk];
+                            F2 += chan_w[c]*eval_2d<M, XY>(qx, qy, qk, rot, v);
+                        }
+                    }
+                }
+                acc2 += w*F2;
+            } else {
+                acc2 += w*eval_2d<M, XY>(qx, qy, qk, rot, v);
+            }
+        }
+    }
+
+    // lanes that share a q: butterfly over the mesh-lane bits
+    #pragma unroll
+    for (int off = LQ; off < 32; off <<= 1) {
+        acc2 += __shfl_xor_sync(FULL_MASK, acc2, off);
+        if constexpr (L::FQ1D) acc1 += __shfl_xor_sync(FULL_MASK, acc1, off);
+    }
+    if (ml == 0) {
+        red[warp][qi][0] = acc2;
+        if constexpr (L::FQ1D) red[warp][qi][1] = acc1;
+    }
+    __syncthreads();
+    if (warp == 0 && ml == 0 && q_ok) {
+        double s2 = 0.0, s1v = 0.0;
+        #pragma unroll
+        for (int k = 0; k < WARPS; ++k) {
+            s2 += red[k][qi][0];
+            if constexpr (L::FQ1D) s1v += red[k][qi][1];
+        }
+        double *out = partial + (size_t)blockIdx.y*L::NOUT*nq;
+        if constexpr (L::FQ1D) {
+            out[2*q_index] = s2;
+            out[2*q_index + 1] = s1v;
+        } else {
+            out[q_index] = s2;
+        }
+    }
+}
+
+// --------------------------------------------------------------- finalize ---
+
+// Sum the mesh splits for each output slot in split order, reduce the
+// segment norms with a fixed tree in the last block, and store (or add, for
+// a call that continues a partly computed mesh) into result.
+template <int UNUSED = 0>
+__global__ void __launch_bounds__(256)
+finalize(int nout_nq, int splits, const double *__restrict__ partial,
+         int nseg, const double *__restrict__ seg_norm,
+         double *__restrict__ result, int accumulate)
+{
+    if (blockIdx.x + 1 < gridDim.x) {
+        const int i = blockIdx.x*256 + threadIdx.x;
+        if (i < nout_nq) {
+            double s = 0.0;
+            for (int k = 0; k < splits; ++k) s += partial[(size_t)k*nout_nq + i];
+            result[i] = accumulate ? result[i] + s : s;
+        }
+        return;
+    }
+    __shared__ double red[4][256];
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int sgi = threadIdx.x; sgi < nseg; sgi += 256) {
+        #pragma unroll
+        for (int k = 0; k < 4; ++k) a[k] += seg_norm[4*sgi + k];
+    }
+    #pragma unroll
+    for (int k = 0; k < 4; ++k) red[k][threadIdx.x] = a[k];
+    for (int s = 128; s > 0; s >>= 1) {
+        __syncthreads();
+        if ((int)threadIdx.x < s) {
+            #pragma unroll
+            for (int k = 0; k < 4; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + s];
+        }
+    }
+    if (threadIdx.x == 0) {
+        #pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            result[nout_nq + k] = accumulate ? result[nout_nq + k] + red[k][0] : red[k][0];
+        }
+    }
+}
+
+}  // namespace sasb200

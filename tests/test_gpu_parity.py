@@ -1,0 +1,221 @@
+"""
+GPU parity: the sm_100a kernels through the C-ABI against the reference DLL
+oracle (oracle/_ref) on identical packed inputs.
+
+Bar (FP64 path): every F^2 slot and norm within rel 1e-12 of the DLL; every
+<F> slot within 1e-12 of its Cauchy-Schwarz scale sqrt(sum w * sum w F^2)
+(see helpers.compare_raw).  The embedded model tests are also checked at the
+reference harness's 5 significant digits.
+"""
+
+import numpy as np
+import pytest
+
+from helpers import (MODELS, RTOL_FP64, compare_raw, golden, interleave,
+                     is_near, load_info, marshal, normalise, nout_of,
+                     reference_raw, variant)
+from sasmodels_b200 import direct_model, load_model, workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_raw(name, q_vectors, pars, cutoff=0.0, reff_mode=0, tile=0):
+    model = load_model(name)
+    kernel = model.make_kernel([np.asarray(v, 'd') for v in q_vectors])
+    kernel.tile = tile
+    details, values, magnetic = marshal(model.info, pars, q_vectors)
+    kernel._call_kernel(details, values, cutoff, magnetic, reff_mode)
+    nout = nout_of(model.info, kernel.dim)
+    nq = kernel.q_input.nq
+    raw = np.concatenate([kernel.result[:nout*nq], kernel.result[nout*nq:nout*nq+4]])
+    return raw, nout, nq, values
+
+
+def assert_parity(name, q_vectors, pars, cutoff=0.0, reff_mode=0, tile=0,
+                  rtol=RTOL_FP64, threads=8):
+    info = load_info(name)
+    ours, nout, nq, values = gpu_raw(name, q_vectors, pars, cutoff, reff_mode, tile)
+    ref = reference_raw(name, info, q_vectors, pars, cutoff, reff_mode,
+                        threads=threads)
+    worst, f2rel = compare_raw(ours, ref, nout, nq, rtol)
+    assert worst <= 1.0, "%s: worst err %.3g x tol (max F^2 rel %.3g)" % (
+        name, worst, f2rel)
+    return ours, ref
+
+
+@pytest.mark.parametrize("name", MODELS)
+def test_golden_dll_cases(cuda, name):
+    """Seeded 1D/2D/magnetic cases recorded from the reference DLL."""
+    info = load_info(name)
+    for case in golden(name)["dll"]:
+        ours, nout, nq, values = gpu_raw(name, case["q"], case["pars"])
+        np.testing.assert_array_equal(values, np.array(case["values"]))
+        worst, f2rel = compare_raw(ours, np.array(case["raw"]), nout, nq)
+        assert worst <= 1.0, (name, case["dim"], worst, f2rel)
+
+
+@pytest.mark.parametrize("name", MODELS)
+def test_model_golden_values(cuda, name):
+    """Each model's embedded test values, through the drop-in API
+    (direct_model.call_kernel / call_Fq on a B200Kernel)."""
+    model = load_model(name)
+    for case in golden(name)["tests"]:
+        qv = [np.asarray(v, 'd') for v in case["q"]]
+        kernel = model.make_kernel(qv)
+        pars = dict(case["pars"])
+        if case["kind"] == "I":
+            out = direct_model.call_kernel(kernel, pars)
+            for t, a in zip(case["y"], out):
+                assert is_near(t, a), (name, case["pars"], t, a)
+        else:
+            F1, F2, reff, shell, ratio = direct_model.call_Fq(kernel, pars)
+            if F1 is not None:
+                for t, a in zip(case["F"], F1):
+                    assert is_near(t, a), (name, "F", t, a)
+            for t, a in zip(case["F2"], F2):
+                assert is_near(t, a), (name, "F2", t, a)
+            assert is_near(case["reff"], reff)
+            assert is_near(case["volume"], shell)
+            assert is_near(case["volume_ratio"], ratio)
+        # and the same points at the FP64 bar against the live oracle
+        pars.pop("radius_effective_mode", None)
+        assert_parity(name, case["q"], pars, threads=1)
+
+
+def test_sphere_config_full(cuda):
+    """sphere 1D headline configuration at full size (1000 q x 35 mesh)."""
+    name, qv, pars = workloads.sphere_1d()
+    assert_parity(name, qv, pars)
+
+
+def test_cylinder_2d_full_mesh_subgrid(cuda):
+    """cylinder 2D oriented: full 490000-point mesh on an 8x8 q block of the
+    256x256 grid."""
+    name, qv, pars = workloads.cylinder_2d_subgrid(8)
+    assert_parity(name, qv, pars)
+
+
+def test_magnetic_full_mesh_subgrid(cuda):
+    """core_shell_sphere magnetic: full 1071-point mesh, 16x16 q block."""
+    name, (qx, qy), pars = workloads.core_shell_sphere_magnetic(n=128)
+    sub = np.arange(0, 128*128, 64)
+    assert_parity(name, [qx[sub], qy[sub]], pars)
+
+
+@pytest.mark.parametrize("k", [0, 1, 2, 3])
+def test_population_members(cuda, k):
+    """Members of the fit population (ellipsoid / core_shell_cylinder 1D
+    with adaptive quadrature), reduced mesh."""
+    pop = workloads.population(n_sets=8, seed=1, max_pd_n=9)
+    name, q, pars = pop[k]
+    assert_parity(name, [q], pars)
+
+
+@pytest.mark.parametrize("tile", [0x00010420, 0x00030408, 0x00020801, 0x00050808, 0x00010801])
+def test_tile_shapes_agree(cuda, tile):
+    """Every tile shape gives the oracle's answer (reduction order differs,
+    the result must not)."""
+    _, qv, pars = workloads.cylinder_2d(n=12, radius_n=7, length_n=5,
+                                        theta_n=5, phi_n=4)
+    assert_parity("cylinder", qv, pars, tile=tile)
+
+
+def test_restart_matches_single_call(cuda):
+    """pd_start/pd_stop restart: two calls over halves of the mesh give the
+    single-call sums (kernel_iq.c:381-423 contract)."""
+    import torch
+    name, qv, pars = workloads.cylinder_2d(n=10, radius_n=5, length_n=5,
+                                           theta_n=4, phi_n=3)
+    model = load_model(name)
+    kernel = model.make_kernel(qv)
+    details, values, magnetic = marshal(model.info, pars, qv)
+    dev_d, dev_v = kernel.upload(details, values)
+    n = details.num_eval
+    with torch.cuda.stream(kernel.stream):
+        full = kernel.launch("Iqxy", dev_d, dev_v, 0, n, 0.0, 0).clone()
+        part = torch.zeros_like(full)
+        kernel.launch("Iqxy", dev_d, dev_v, 0, n//3, 0.0, 0, result_dev=part)
+        kernel.launch("Iqxy", dev_d, dev_v, n//3, n, 0.0, 0, result_dev=part)
+    kernel.stream.synchronize()
+    full = full.cpu().numpy()
+    part = part.cpu().numpy()
+    nq = kernel.q_input.nq
+    worst, _ = compare_raw(part[:nq+4], full[:nq+4], 1, nq, 1e-13)
+    assert worst <= 1.0
+
+
+def test_cutoff_and_reff(cuda):
+    """cutoff > 0 drops light mesh points; R_eff accumulated when asked."""
+    name = "cylinder"
+    q = np.logspace(-3, -0.5, 50)
+    pars = dict(radius=30., radius_pd=0.2, radius_pd_n=25, length=200.,
+                length_pd=0.3, length_pd_n=25)
+    assert_parity(name, [q], pars, cutoff=1e-4, reff_mode=1)
+    assert_parity(name, [q], pars, cutoff=0.0, reff_mode=7)
+
+
+def test_deterministic(cuda):
+    name, qv, pars = workloads.sphere_1d(nq=333)
+    a, *_ = gpu_raw(name, qv, pars)
+    b, *_ = gpu_raw(name, qv, pars)
+    np.testing.assert_array_equal(a, b)
+
+
+def test_edge_cases(cuda):
+    """single q, monodisperse (mesh of one), q = 0 in the magnetic kernel,
+    empty mesh range."""
+    assert_parity("sphere", [np.array([0.05])], dict(radius=80.), threads=1)
+    assert_parity("cylinder", [np.array([0.0, 1e-3]), np.array([0.0, 2e-3])],
+                  dict(theta=30., phi=10.), threads=1)
+    _, qv, pars = workloads.core_shell_sphere_magnetic(n=3, radius_n=3, thickness_n=3)
+    assert abs(qv[0][4]) + abs(qv[1][4]) == 0.0  # grid centre is q = 0
+    assert_parity("core_shell_sphere", qv, pars, threads=1)
+    # empty mesh range: sums are zero
+    import torch
+    model = load_model("sphere")
+    kernel = model.make_kernel([np.array([0.1, 0.2])])
+    details, values, _ = marshal(model.info, dict(radius_pd=0.1, radius_pd_n=5),
+                                 [np.array([0.1, 0.2])])
+    dev_d, dev_v = kernel.upload(details, values)
+    with torch.cuda.stream(kernel.stream):
+        res = kernel.launch("Iq", dev_d, dev_v, 0, 0, 0.0, 0)
+    kernel.stream.synchronize()
+    assert not res.cpu().numpy().any()
+
+
+def test_small_workspace_chunks(cuda):
+    """A workspace smaller than the mesh is processed in chunks with the same
+    answer."""
+    import torch
+    name, qv, pars = workloads.cylinder_2d(n=8, radius_n=9, length_n=9,
+                                           theta_n=5, phi_n=5)
+    model = load_model(name)
+    kernel = model.make_kernel(qv)
+    details, values, magnetic = marshal(model.info, pars, qv)
+    dev_d, dev_v = kernel.upload(details, values)
+    n = details.num_eval
+    full_ws = model.lib.workspace_bytes("Iqxy", kernel.q_input.nq, n, 0)
+    small = torch.empty(full_ws//5, dtype=torch.uint8, device=kernel.device)
+    out = torch.zeros(kernel.q_input.nq + 4, dtype=torch.float64, device=kernel.device)
+    with torch.cuda.stream(kernel.stream):
+        ref = kernel.launch("Iqxy", dev_d, dev_v, 0, n, 0.0, 0).clone()
+        model.lib.call("Iqxy", kernel.q_input.nq, 0, n, dev_d.data_ptr(),
+                       dev_v.data_ptr(), kernel.q_input.q_dev.data_ptr(),
+                       out.data_ptr(), 0.0, 0, small.data_ptr(), small.numel(), 0,
+                       kernel.stream.cuda_stream)
+    kernel.stream.synchronize()
+    worst, _ = compare_raw(out.cpu().numpy(), ref.cpu().numpy()[:kernel.q_input.nq+4],
+                           1, kernel.q_input.nq, 1e-13)
+    assert worst <= 1.0
+
+
+def test_iq_device_matches_host(cuda):
+    name, qv, pars = workloads.sphere_1d(nq=200)
+    model = load_model(name)
+    kernel = model.make_kernel(qv)
+    host = direct_model.call_kernel(kernel, pars)
+    details, values, magnetic = marshal(model.info, pars, qv)
+    dev_d, dev_v = kernel.upload(details, values)
+    dev = kernel.Iq_device(dev_d, dev_v, details.num_eval, values[0], values[1])
+    kernel.stream.synchronize()
+    np.testing.assert_allclose(dev.cpu().numpy(), host, rtol=1e-14)

@@ -1,0 +1,168 @@
+"""
+CPU tests: the host-side mirror of the reference call path, the oracle pinned
+against the reference's golden vectors, and the C-ABI libraries' exports.
+No GPU is touched here.
+"""
+
+import ctypes as ct
+import os
+import re
+
+import numpy as np
+import pytest
+
+from helpers import (MODELS, golden, interleave, is_near, load_info, marshal,
+                     normalise, nout_of, variant)
+from sasmodels_b200 import _abi, weights
+from sasmodels_b200.generate import device_source, find_xy_mode
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+
+
+@pytest.mark.parametrize("name", MODELS)
+def test_marshal_matches_reference(name):
+    """get_mesh + make_kernel_args reproduce the reference's packed arrays."""
+    info = load_info(name)
+    for case in golden(name)["marshal"]:
+        details, values, magnetic = marshal(info, case["pars"], case["q"])
+        np.testing.assert_array_equal(details.buffer, case["details"])
+        np.testing.assert_array_equal(values, np.array(case["values"]))
+        assert magnetic == case["magnetic"]
+
+
+@pytest.mark.parametrize("name", MODELS)
+def test_oracle_reproduces_reference_dll(name):
+    """oracle/_ref gives bitwise the raw vectors the reference's own
+    DllKernel produced on the same inputs."""
+    from oracle import refdll
+    info = load_info(name)
+    dll = refdll.load(name)
+    for case in golden(name)["dll"]:
+        nout = nout_of(info, case["dim"])
+        raw = dll.call(variant(case["dim"], case["magnetic"]),
+                       interleave(case["q"]), case["details"],
+                       np.array(case["values"]), nout)
+        np.testing.assert_array_equal(raw, np.array(case["raw"]))
+
+
+@pytest.mark.parametrize("name", MODELS)
+def test_oracle_against_model_golden_tests(name):
+    """The oracle meets each model's embedded test values at 5 significant
+    digits (the reference harness rule, model_test.py:443-471)."""
+    info = load_info(name)
+    from helpers import reference_raw
+    for case in golden(name)["tests"]:
+        pars = dict(case["pars"])
+        reff_mode = int(pars.pop("radius_effective_mode", 1 if case["kind"] == "Fq" else 0))
+        raw = reference_raw(name, info, case["q"], pars, reff_mode=reff_mode)
+        details, values, _ = marshal(info, pars, case["q"])
+        nq = len(case["q"][0])
+        out = normalise(raw, nout_of(info, case["dim"]), nq, values)
+        if case["kind"] == "I":
+            for t, a in zip(case["y"], out["I"]):
+                assert is_near(t, a), (name, case, t, a)
+        else:
+            if out["F1"] is not None:
+                for t, a in zip(case["F"], out["F1"]):
+                    assert is_near(t, a), (name, "F", t, a)
+            for t, a in zip(case["F2"], out["F2"]):
+                assert is_near(t, a), (name, "F2", t, a)
+            assert is_near(case["reff"], out["reff"])
+            assert is_near(case["volume"], out["shell"])
+            assert is_near(case["volume_ratio"], out["ratio"])
+
+
+def test_weights_normalised_and_truncated():
+    v, w = weights.get_weights("gaussian", 35, 0.1, 3, 50.0, (0, np.inf), True)
+    assert len(v) == 35 and abs(w.sum() - 1) < 1e-15
+    assert v.min() == pytest.approx(35.0) and v.max() == pytest.approx(65.0)
+    # truncation at the lower limit
+    v, w = weights.get_weights("gaussian", 35, 0.5, 3, 1.0, (0, np.inf), True)
+    assert v.min() >= 0 and len(v) < 35
+    # orientation jitter is absolute and centred on zero
+    v, w = weights.get_weights("gaussian", 5, 10.0, 3, 60.0, (-180, 180), False)
+    assert v[len(v)//2] == 0.0
+
+
+def test_too_many_polydisperse_parameters():
+    from sasmodels_b200.details import make_details
+    info = load_info("sphere")
+    with pytest.raises(ValueError):
+        make_details(info, np.array([2, 2, 2]), np.array([0, 2, 4]), 6)
+
+
+def test_device_source_lexer():
+    code = """
+// comment with double foo(
+static double f(double x) { constant double *w = T; return x*w[0]; }
+constant double T[2] = {1.0, 2.0};
+double g(double);
+typedef struct { double a; } S;
+#define X(a) (a)
+double sas_3j1x_x(double q)
+{
+    if (q < 0) { return 1.0; }
+    return q;
+}
+"""
+    out = device_source(code)
+    assert "__device__ static double f(double x) { const double *w" in out
+    assert "__device__ const double T[2]" in out
+    assert "__device__ double g(double);" in out
+    assert "typedef struct { double a; } S;" in out
+    assert "__device__ double sas_3j1x_x(double q)" in out
+    assert "#define X(a) (a)" in out
+    assert find_xy_mode(["double Iqac(double qab, double qc)"]) == "qac"
+    assert find_xy_mode(["static double Iq(double q)"]) == "qa"
+
+
+def _header_suffixes():
+    text = open(os.path.join(ROOT, "include", "sasb200.h")).read()
+    block = text[text.index("#define SASB200_DECLARE_MODEL"):]
+    block = block[:block.index("SASB200_DECLARE_MODEL(sphere)")]
+    return sorted(set(re.findall(r"sasb200_##M##_(\w+)\(", block)))
+
+
+def test_header_declares_models():
+    text = open(os.path.join(ROOT, "include", "sasb200.h")).read()
+    for name in MODELS:
+        assert "SASB200_DECLARE_MODEL(%s)" % name in text
+
+
+@pytest.mark.parametrize("name", MODELS)
+def test_library_exports_header_symbols(name):
+    """Each built library loads without a GPU and exports every symbol the
+    header declares for it."""
+    path = _abi.library_path(name)
+    assert os.path.exists(path), "library not built: %s" % path
+    lib = ct.CDLL(path)
+    for suffix in _header_suffixes():
+        getattr(lib, "sasb200_%s_%s" % (name, suffix))
+    meta = _abi.load_metadata(name)
+    assert meta["id"] == name
+
+
+@pytest.mark.parametrize("name", MODELS)
+def test_abi_host_queries(name):
+    """Size and tile queries run on the host (no kernel launch)."""
+    lib = _abi.load_library(name)
+    shapes = lib.tile_shapes()
+    assert len(shapes) >= 1 and all(s & 0xff in (1, 8, 32) for s in shapes)
+    n = lib.workspace_bytes("Iq", 1000, 35)
+    assert n >= 35*8 and n % 256 == 0
+    assert lib.workspace_bytes("Iqxy", 65536, 490000, 0) > 490000*8
+    tile = lib.default_tile(1000, 35)
+    assert (tile & 0xff) in (1, 8, 32)
+
+
+def test_abi_rejects_bad_arguments_without_gpu():
+    """Argument checks happen before any CUDA call."""
+    lib = _abi.load_library("sphere")
+    with pytest.raises(RuntimeError, match="pd_start"):
+        lib.call("Iq", 10, 5, 3, 1, 1, 1, 1, 0.0, 0, 1, 1 << 20, 0, None)
+    with pytest.raises(RuntimeError, match="null"):
+        lib.call("Iq", 10, 0, 3, None, 1, 1, 1, 0.0, 0, 1, 1 << 20, 0, None)
+    with pytest.raises(RuntimeError, match="tile"):
+        lib.call("Iq", 10, 0, 3, 1, 1, 1, 1, 0.0, 0, 1, 1 << 20, 0x10307, None)
+    with pytest.raises(RuntimeError, match="workspace"):
+        lib.call("Iq", 10, 0, 3, 1, 1, 1, 1, 0.0, 0, 1, 16, 0, None)
