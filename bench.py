@@ -49,10 +49,10 @@ def host_threads():
         return os.cpu_count() or 1
 
 
-def workload(config):
+def workload(config, grid=256):
     from sasmodels_b200 import workloads
     if config == "cylinder2d":
-        return workloads.cylinder_2d(), "cylinder 2D oriented FP64, 256x256 q, R(35) x L(35) x theta(20) x phi(20) mesh"
+        return workloads.cylinder_2d(n=grid), "cylinder 2D oriented FP64, %dx%d q, R(35) x L(35) x theta(20) x phi(20) mesh" % (grid, grid)
     if config == "sphere1d":
         return workloads.sphere_1d(), "sphere 1D FP64, 1000 log q, R gaussian pd 0.1 x 35"
     if config == "magnetic":
@@ -211,7 +211,7 @@ def run_reference(args, world, rank):
         if step >= args.warmup:
             values.append(v)
     value = statistics.median(values)
-    (_, _, _), desc = workload(args.config)
+    (_, _, _), desc = workload(args.config, args.grid)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -232,7 +232,7 @@ def run_b200(args, world, rank, local):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    (name, qv, pars), desc = workload(args.config)
+    (name, qv, pars), desc = workload(args.config, args.grid)
     model = load_model(name, device=dev)
     kernel = model.make_kernel(qv)
     details, values, magnetic = marshal(model.info, pars, qv)
@@ -344,6 +344,8 @@ def main(argv=None):
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="cylinder2d",
                     choices=["cylinder2d", "sphere1d", "magnetic"])
+    ap.add_argument("--grid", type=int, default=256,
+                    help="q grid edge for cylinder2d (smaller for profiling)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args(argv)

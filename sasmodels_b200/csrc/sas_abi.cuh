@@ -150,7 +150,8 @@ __host__ uint64_t workspace_bytes(int32_t nq, int32_t n_mesh, int32_t tile_code)
 {
     if (nq < 0 || n_mesh < 0) return 0;
     Tile t = tile_code ? tile_decode(tile_code) : choose_tile(nq, n_mesh);
-    const long long chunk = n_mesh < (1 << 20) ? n_mesh : (1 << 20);
+    // at least one segment, at most 2^20 mesh points per pass
+    const long long chunk = n_mesh < 1 ? 1 : (n_mesh < (1 << 20) ? n_mesh : (1 << 20));
     return Workspace<M, VAR>(nq, chunk, t.splits).total;
 }
 
