@@ -331,9 +331,11 @@ def run_b200(args, world, rank, local):
 #: from the ncu instruction counters of iq_main (2*DFMA + DADD + DMUL per
 #: thread instruction) divided by the evaluations of the captured launch;
 #: see profiles/.
-FLOPS_PER_EVAL = {}
-#: dram read+write bytes of the dominant kernel per step (ncu), or None
-TRAFFIC_PER_STEP = {}
+FLOPS_PER_EVAL = {"cylinder2d": 160.8}
+#: dram read+write bytes of the dominant kernel per launch (ncu): the mesh
+#: table is read once from DRAM and then served from L2; it does not grow
+#: with the number of q points (profiles/iq_main_cylinder2d.md)
+TRAFFIC_PER_STEP = {"cylinder2d": 39.36e6}
 
 
 def main(argv=None):
