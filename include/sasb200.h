@@ -82,6 +82,27 @@ extern "C" {
 
 SASB200_DECLARE_MODEL(sphere)
 SASB200_DECLARE_MODEL(cylinder)
+
+/*
+ * Allocation-free variant of sasb200_cylinder_Iqxy.  No counterpart in the
+ * reference: it is for callers that may not allocate GPU memory (plugins
+ * running inside another program's CUDA context or allocator lock, real-time
+ * loops).  Same arguments as sasb200_cylinder_Iqxy without workspace and
+ * workspace_bytes; the scratch comes from a static 8 MiB device array in the
+ * library (SASB200_NOALLOC_SCRATCH_BYTES), held on every GPU that loads the
+ * library until the process exits.  The first call on each device looks up
+ * the array's device address (cudaGetSymbolAddress, may load the module):
+ * make it before any stream capture.  Problems whose scratch for one
+ * 128-point mesh segment exceeds the array (very large nq) return -2 with a
+ * message; larger meshes are processed in chunks.  All calls share the
+ * array: calls that overlap on the GPU race, so keep them on one stream.
+ */
+#define SASB200_NOALLOC_SCRATCH_BYTES (8ull << 20)
+int32_t sasb200_cylinder_Iqxy_noalloc(
+    int32_t nq, int32_t pd_start, int32_t pd_stop, const int32_t *details,
+    const double *values, const double *q, double *result, double cutoff,
+    int32_t radius_effective_mode, int32_t tile, void *stream);
+
 SASB200_DECLARE_MODEL(core_shell_sphere)
 SASB200_DECLARE_MODEL(ellipsoid)
 SASB200_DECLARE_MODEL(core_shell_cylinder)

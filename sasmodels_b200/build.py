@@ -80,7 +80,8 @@ def build_model(name, force=False, verbose=False, extra_flags=()):
     tag = generate.source_tag(src + " ".join(flags)
                               + _read(os.path.join(CSRC, "sas_driver.cuh"))
                               + _read(os.path.join(CSRC, "sas_abi.cuh"))
-                              + _read(os.path.join(CSRC, "sas_device.cuh")))
+                              + _read(os.path.join(CSRC, "sas_device.cuh"))
+                              + _read(os.path.join(CSRC, "sas_noalloc.cuh")))
     meta["build_tag"] = tag
     os.makedirs(LIB, exist_ok=True)
     os.makedirs(BUILD, exist_ok=True)

@@ -33,6 +33,10 @@ CSRC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc")
 # xy mode codes shared with sas_driver.cuh
 XY_CODES = {"qa": 1, "qac": 2, "qabc": 3, "qxy": 4}
 
+#: models whose library also exports the allocation-free entry point
+#: sasb200_<model>_<variant>_noalloc (csrc/sas_noalloc.cuh)
+NOALLOC_EXPORTS = {"cylinder": ("Iqxy", "sasb200::VAR_IQXY")}
+
 _IQXY_RE = re.compile(r"(^|\s)double\s+I(?P<mode>q(ac|abc|xy))\s*[(]", re.M)
 _SHELL_RE = re.compile(r"(^|\s)double\s+shell_volume\s*[(]", re.M)
 _IDENT_RE = re.compile(r"(?<![.0-9A-Za-z_])([A-Za-z_][A-Za-z0-9_]*)")
@@ -346,6 +350,11 @@ def make_cuda_source(sm_info, sources):
     body.append('#include "sas_driver.cuh"')
     body.append('#include "sas_abi.cuh"')
     body.append("SASB200_EXPORT_MODEL(%s, sasm::SasModel)" % sm_info.id)
+    if sm_info.id in NOALLOC_EXPORTS:
+        variant, var = NOALLOC_EXPORTS[sm_info.id]
+        body.append('#include "sas_noalloc.cuh"')
+        body.append("SASB200_EXPORT_NOALLOC(%s, sasm::SasModel, %s, %s)"
+                    % (sm_info.id, variant, var))
     meta = _mi.from_sasmodels(sm_info, xy_mode, have_shell)
     meta["tests"] = _jsonable_tests(getattr(sm_info, "tests", None) or [])
     return "\n".join(body) + "\n", meta
