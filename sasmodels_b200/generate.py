@@ -144,11 +144,35 @@ def _emit(stmt):
         body = "".join("const" if (k == "ident" and t == "constant") else t
                        for k, t in stmt)
         return "__device__ " + body
-    # file-scope data
+    # file-scope data: small tables (polynomial coefficients, the 20- to
+    # 150-point Gauss rules) go to __constant__ memory, where warp-uniform
+    # reads are served by the constant cache; large tables (500- and
+    # 5000-point rules) to global memory
     if "constant" in words:
-        return "".join("__device__ const" if (k == "ident" and t == "constant")
+        space = "__constant__ const" if _table_size(stmt) <= CONSTANT_TABLE_MAX \
+            else "__device__ const"
+        return "".join(space if (k == "ident" and t == "constant")
                        else t for k, t in stmt)
     return "__device__ " + "".join(t for _, t in stmt)
+
+
+#: largest file-scope table (elements) placed in __constant__ memory
+CONSTANT_TABLE_MAX = 256
+
+
+def _table_size(stmt):
+    """Declared element count of a file-scope array ([] counts as small)."""
+    toks = [t for k, t in stmt if k not in ("ws", "comment")]
+    if "[" not in toks:
+        return 1
+    i = toks.index("[")
+    inner = toks[i + 1:toks.index("]", i)]
+    if not inner:
+        return 0
+    try:
+        return int(inner[0]) if len(inner) == 1 else 1 << 30
+    except ValueError:
+        return 1 << 30
 
 
 # ------------------------------------------------------------ model struct ---

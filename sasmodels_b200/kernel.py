@@ -51,25 +51,54 @@ def _require_cuda(device):
     return dev
 
 
+def locality_order(qx, qy, bits=10):
+    """
+    Permutation that walks the (qx, qy) points along a Morton (Z-order) curve
+    of the plane, so the 32 points a warp takes are close together.  Nearby
+    points see nearby |q|, q_ab and q_c for every orientation, so the lanes of
+    a warp follow the same branches of the model (J1 series vs asymptotic,
+    adaptive quadrature order) instead of diverging.
+    """
+    def quantise(v):
+        lo, hi = float(v.min()), float(v.max())
+        scale = (2**bits - 1)/(hi - lo) if hi > lo else 0.0
+        return np.rint((v - lo)*scale).astype(np.uint64)
+    ix, iy = quantise(qx), quantise(qy)
+    code = np.zeros(len(qx), np.uint64)
+    for b in range(bits):
+        code |= ((ix >> np.uint64(b)) & np.uint64(1)) << np.uint64(2*b)
+        code |= ((iy >> np.uint64(b)) & np.uint64(1)) << np.uint64(2*b + 1)
+    return np.argsort(code, kind="stable")
+
+
 class QInput:
     """q points for one kernel: 1D ``q`` or interleaved ``(qx, qy)`` pairs,
-    uploaded once (``kernelcuda.py:386-422`` does the same per make_kernel)."""
+    uploaded once (``kernelcuda.py:386-422`` does the same per make_kernel).
+    2D points are uploaded in :func:`locality_order` (``order[i]`` is the
+    caller's index of device slot i); results are put back in caller order."""
 
-    def __init__(self, q_vectors, device):
+    def __init__(self, q_vectors, device, reorder=True):
         torch = _torch()
         q_vectors = [np.ascontiguousarray(v, 'd').ravel() for v in q_vectors]
         self.q_vectors = q_vectors
         self.nq = int(q_vectors[0].size)
         self.is_2d = len(q_vectors) == 2
+        self.order = None
         if self.is_2d:
+            qx, qy = q_vectors
+            if reorder and self.nq > 32:
+                self.order = locality_order(qx, qy)
+                qx, qy = qx[self.order], qy[self.order]
             q = np.empty(2*self.nq, 'd')
-            q[0::2] = q_vectors[0]
-            q[1::2] = q_vectors[1]
+            q[0::2] = qx
+            q[1::2] = qy
         elif len(q_vectors) == 1:
             q = q_vectors[0]
         else:
             raise ValueError("q_vectors must be [q] or [qx, qy]")
         self.q = q
+        self.order_dev = (torch.as_tensor(self.order, device=device)
+                          if self.order is not None else None)
         self.dtype = np.dtype('d')
         self.q_dev = torch.as_tensor(q, device=device) if self.nq else \
             torch.zeros(2, dtype=torch.float64, device=device)
@@ -93,8 +122,8 @@ class B200Model(_KernelModelBase):
         self.device = device
         self.lib = _abi.load_library(model_info.id, lib_dir)
 
-    def make_kernel(self, q_vectors):
-        return B200Kernel(self, q_vectors)
+    def make_kernel(self, q_vectors, reorder=True):
+        return B200Kernel(self, q_vectors, reorder=reorder)
 
     def release(self):
         pass
@@ -103,7 +132,7 @@ class B200Model(_KernelModelBase):
 class B200Kernel(_KernelBase):
     """Callable kernel bound to one set of q points."""
 
-    def __init__(self, model, q_vectors, device=None):
+    def __init__(self, model, q_vectors, device=None, reorder=True):
         torch = _torch()
         self.model = model
         self.info = model.info
@@ -111,7 +140,7 @@ class B200Kernel(_KernelBase):
         self.device = _require_cuda(device if device is not None else model.device)
         self.stream = torch.cuda.Stream(self.device)
         with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
-            self.q_input = QInput(q_vectors, self.device)
+            self.q_input = QInput(q_vectors, self.device, reorder)
             self.dim = '2d' if self.q_input.is_2d else '1d'
             nq = self.q_input.nq
             nout = 2 if self.info.have_Fq else 1
@@ -202,6 +231,10 @@ class B200Kernel(_KernelBase):
             self._result_pin[:n].copy_(self._result_dev, non_blocking=True)
         self.stream.synchronize()
         self.result[:] = self._result_pin.numpy()
+        order = self.q_input.order
+        if order is not None:
+            nq = self.q_input.nq
+            self.result[order] = self._result_pin.numpy()[:nq]
 
     # ------------------------------------------- reference engine interface --
     def Iq(self, call_details, values, cutoff, magnetic):
@@ -252,6 +285,8 @@ class B200Kernel(_KernelBase):
             shell = torch.where(shell == 0, torch.ones_like(shell), shell)
             F2 = res[0:nout*nq:nout]/total
             I = (scale/shell)*F2 + background
+            if self.q_input.order_dev is not None:
+                I = torch.empty_like(I).index_copy_(0, self.q_input.order_dev, I)
             if out is not None:
                 out.copy_(I)
                 return out

@@ -96,6 +96,7 @@ def test_device_source_lexer():
 // comment with double foo(
 static double f(double x) { constant double *w = T; return x*w[0]; }
 constant double T[2] = {1.0, 2.0};
+constant double BIG[5000] = {1.0};
 double g(double);
 typedef struct { double a; } S;
 #define X(a) (a)
@@ -107,7 +108,8 @@ double sas_3j1x_x(double q)
 """
     out = device_source(code)
     assert "__device__ static double f(double x) { const double *w" in out
-    assert "__device__ const double T[2]" in out
+    assert "__constant__ const double T[2]" in out
+    assert "__device__ const double BIG[5000]" in out
     assert "__device__ double g(double);" in out
     assert "typedef struct { double a; } S;" in out
     assert "__device__ double sas_3j1x_x(double q)" in out
