@@ -107,6 +107,21 @@ SASB200_DECLARE_MODEL(core_shell_sphere)
 SASB200_DECLARE_MODEL(ellipsoid)
 SASB200_DECLARE_MODEL(core_shell_cylinder)
 
+/*
+ * FP32-compensated form of the same five models, exported from the same
+ * libraries under the prefix <model>_f32c: identical arguments and result
+ * layout; the amplitude arithmetic runs in FP32 (and the MUFU unit) with
+ * FP64 phases, FP64 quadrature and dispersity sums and FP64 volumes.
+ * Counterpart of the reference's single-precision build of the same kernels
+ * (generate.py:449-488 convert_type, FP32 branches of sas_J1.c:155-231 and
+ * sas_3j1x_x.c:40-44); max relative error vs the FP64 DLL <= 1e-5.
+ */
+SASB200_DECLARE_MODEL(sphere_f32c)
+SASB200_DECLARE_MODEL(cylinder_f32c)
+SASB200_DECLARE_MODEL(core_shell_sphere_f32c)
+SASB200_DECLARE_MODEL(ellipsoid_f32c)
+SASB200_DECLARE_MODEL(core_shell_cylinder_f32c)
+
 #ifdef __cplusplus
 }
 #endif

@@ -45,7 +45,9 @@ def available_models(lib_dir=None):
 
 
 class ModelLib:
-    """The exported functions of one ``libsasb200_<name>.so``."""
+    """The exported functions of one ``libsasb200_<model>.so`` under one
+    symbol prefix: ``<model>`` for the FP64 form, ``<model>_f32c`` for the
+    FP32-compensated form of the same library."""
 
     def __init__(self, name, path=None):
         self.name = name
@@ -101,10 +103,12 @@ class ModelLib:
                 self.name, variant, status, self.last_error()))
 
 
-def load_library(name, lib_dir=None):
-    key = (name, lib_dir)
+def load_library(name, lib_dir=None, form="double"):
+    """Entry points of model *name*; *form* is "double" or "float32c"."""
+    key = (name, lib_dir, form)
     if key not in _LOADED:
-        _LOADED[key] = ModelLib(name, library_path(name, lib_dir))
+        prefix = name if form == "double" else name + "_f32c"
+        _LOADED[key] = ModelLib(prefix, library_path(name, lib_dir))
     return _LOADED[key]
 
 

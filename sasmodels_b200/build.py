@@ -81,7 +81,9 @@ def build_model(name, force=False, verbose=False, extra_flags=()):
                               + _read(os.path.join(CSRC, "sas_driver.cuh"))
                               + _read(os.path.join(CSRC, "sas_abi.cuh"))
                               + _read(os.path.join(CSRC, "sas_device.cuh"))
-                              + _read(os.path.join(CSRC, "sas_noalloc.cuh")))
+                              + _read(os.path.join(CSRC, "sas_noalloc.cuh"))
+                              + _read(os.path.join(CSRC, "fp32c_math.cuh"))
+                              + _read(os.path.join(CSRC, "fp32c_models.cuh")))
     meta["build_tag"] = tag
     os.makedirs(LIB, exist_ok=True)
     os.makedirs(BUILD, exist_ok=True)

@@ -49,10 +49,7 @@ def build_model(model_info, dtype=None, platform=PLATFORM, device=None):
             from . import build
             build.build_model(name)
         info = load_model_info(name)
-    if dtype in ("single", "float32", "f", "float32c", "single!"):
-        from .fp32c import B200ModelF32c
-        return B200ModelF32c(info, device=device)
-    return B200Model(info, dtype="double", device=device)
+    return B200Model(info, dtype=dtype, device=device)
 
 
 _ORIGINAL = {}

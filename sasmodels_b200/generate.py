@@ -371,17 +371,109 @@ def make_cuda_source(sm_info, sources):
         body.append(device_source(fn))
     body.append(model_struct(sm_info, table, xy_mode, have_shell))
     body.append("}  // namespace sasm")
+    f32c = f32c_block(sm_info.id, table, codes)
+    if f32c:
+        body.append(f32c)
     body.append('#include "sas_driver.cuh"')
     body.append('#include "sas_abi.cuh"')
     body.append("SASB200_EXPORT_MODEL(%s, sasm::SasModel)" % sm_info.id)
+    if f32c:
+        body.append("SASB200_EXPORT_MODEL(%s_f32c, sasm::SasModelF32c)" % sm_info.id)
     if sm_info.id in NOALLOC_EXPORTS:
         variant, var = NOALLOC_EXPORTS[sm_info.id]
         body.append('#include "sas_noalloc.cuh"')
         body.append("SASB200_EXPORT_NOALLOC(%s, sasm::SasModel, %s, %s)"
                     % (sm_info.id, variant, var))
     meta = _mi.from_sasmodels(sm_info, xy_mode, have_shell)
-    meta["tests"] = _jsonable_tests(getattr(sm_info, "tests", None) or [])
+    meta["f32c"] = bool(f32c)
     return "\n".join(body) + "\n", meta
+
+
+# ------------------------------------------------------ FP32c bindings ---
+
+#: models with hand-written FP32-compensated physics (csrc/fp32c_models.cuh):
+#: expected kernel parameter order and the binding of fq/iqac to it
+F32C_MODELS = {
+    "sphere": (["sld", "sld_solvent", "radius"],
+               "f32c::sphere_fq(q, v[0], v[1], v[2], F1, F2);", None),
+    "core_shell_sphere": (["radius", "thickness", "sld_core", "sld_shell", "sld_solvent"],
+                          "f32c::core_shell_sphere_fq(q, v[0], v[1], v[2], v[3], v[4], F1, F2);",
+                          None),
+    "cylinder": (["sld", "sld_solvent", "radius", "length", "theta", "phi"],
+                 "f32c::cylinder_fq(q, v[0], v[1], v[2], v[3], F1, F2);",
+                 "return f32c::cylinder_iqac(qab, qc, v[0], v[1], v[2], v[3]);"),
+    "ellipsoid": (["sld", "sld_solvent", "radius_polar", "radius_equatorial", "theta", "phi"],
+                  "f32c::ellipsoid_fq(q, v[0], v[1], v[2], v[3], F1, F2);",
+                  "return f32c::ellipsoid_iqac(qab, qc, v[0], v[1], v[2], v[3]);"),
+    "core_shell_cylinder": (["sld_core", "sld_shell", "sld_solvent", "radius", "thickness",
+                             "length", "theta", "phi"],
+                            "f32c::core_shell_cylinder_fq(q, v[0], v[1], v[2], v[3], v[4], v[5], F1, F2);",
+                            "return f32c::core_shell_cylinder_iqac(qab, qc, v[0], v[1], v[2], v[3], v[4], v[5]);"),
+}
+
+_GAUSS_RE = re.compile(r"constant\s+double\s+Gauss(\d+)(Z|Wt)\s*\[\s*\d*\s*\]\s*=\s*\{(.*?)\}", re.S)
+_RULES = (20, 76, 500, 5000)
+_M_PI_4 = 0.7853981633974483     # kernel_header.c literal
+
+
+def gauss_tables(codes):
+    """{n: (z, w)} parsed from the plugin's quadrature sources."""
+    import numpy as np
+    found = {}
+    for code in codes:
+        for m in _GAUSS_RE.finditer(code):
+            n, kind, body = int(m.group(1)), m.group(2), m.group(3)
+            body = re.sub(r"//[^\n]*", "", body)
+            vals = [float(t) for t in body.replace("\n", " ").split(",") if t.strip()]
+            found.setdefault(n, {})[kind] = np.array(vals[:n])
+    return {n: (d["Z"], d["Wt"]) for n, d in found.items() if "Z" in d and "Wt" in d}
+
+
+def _c_array(name, vals):
+    return "__device__ const double %s[%d] = {%s};" % (
+        name, len(vals), ",".join(repr(float(v)) for v in vals))
+
+
+def f32c_block(name, table, codes):
+    """FP32c binding struct for a model listed in F32C_MODELS, or '' if the
+    model has no FP32c physics (or its parameter table changed)."""
+    import numpy as np
+    if name not in F32C_MODELS:
+        return ""
+    expected, fq, iqac = F32C_MODELS[name]
+    if [p.id for p in table.kernel_parameters] != expected:
+        raise ValueError("FP32c binding for %s expects parameters %s" % (name, expected))
+    out = ['#include "fp32c_models.cuh"', "namespace sasm {"]
+    rules = gauss_tables(codes)
+    if all(n in rules for n in _RULES):
+        for n in _RULES:
+            z, w = rules[n]
+            theta = z*_M_PI_4 + _M_PI_4
+            out.append(_c_array("F32cZ%d" % n, z))
+            out.append(_c_array("F32cW%d" % n, w))
+            out.append(_c_array("F32cSin%d" % n, np.sin(theta)))
+            out.append(_c_array("F32cCos%d" % n, np.cos(theta)))
+    out.append("}  // namespace sasm")
+    out.append("namespace f32c {")
+    out.append("__device__ __forceinline__ Rule rule_for(double qr) {")
+    if all(n in rules for n in _RULES):
+        out.append("  if (qr < 10) return Rule{20, sasm::F32cZ20, sasm::F32cW20, sasm::F32cSin20, sasm::F32cCos20};")
+        out.append("  if (qr < 100) return Rule{76, sasm::F32cZ76, sasm::F32cW76, sasm::F32cSin76, sasm::F32cCos76};")
+        out.append("  if (qr < 750) return Rule{500, sasm::F32cZ500, sasm::F32cW500, sasm::F32cSin500, sasm::F32cCos500};")
+        out.append("  return Rule{5000, sasm::F32cZ5000, sasm::F32cW5000, sasm::F32cSin5000, sasm::F32cCos5000};")
+    else:
+        out.append("  return Rule{0, nullptr, nullptr, nullptr, nullptr};")
+    out.append("}")
+    out.append("}  // namespace f32c")
+    out.append("namespace sasm {")
+    out.append("struct SasModelF32c : SasModel {")
+    out.append("  __device__ static void fq(double q, double &F1, double &F2, const double *v) { %s }" % fq)
+    out.append("  __device__ static double iq(double q, const double *v) { double F1, F2; fq(q, F1, F2, v); return F2; }")
+    if iqac:
+        out.append("  __device__ static double iqac(double qab, double qc, const double *v) { %s }" % iqac)
+    out.append("};")
+    out.append("}  // namespace sasm")
+    return "\n".join(out)
 
 
 def _jsonable_tests(tests):

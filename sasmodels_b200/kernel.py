@@ -107,20 +107,33 @@ class QInput:
         self.q_dev = None
 
 
+FP64_NAMES = (None, "double", "d", "float64", np.float64, "double!")
+FP32C_NAMES = ("single", "float", "f", "float32", np.float32, "float32c", "single!", "fast")
+
+
 class B200Model(_KernelModelBase):
     """
     Compute engine for one model on one CUDA device.
 
-    *dtype* is ``"double"`` (the FP64 path built from the model's own C).
+    *dtype* selects the form: ``"double"`` runs the model plugin's own C in
+    FP64; ``"float32c"`` (also accepted as ``"single"``/``"float32"``, the
+    reference's single-precision names) runs the hand-written FP32-compensated
+    physics where the model has it: FP32 bulk arithmetic, FP64 phases and
+    FP64 sums.  Models without FP32c physics run the FP64 form for either.
+    Results are always float64 arrays.
     """
     def __init__(self, model_info, dtype="double", device=None, lib_dir=None):
         self.info = model_info
-        dtype = "double" if dtype in (None, "double", "d", "float64", np.float64) else dtype
-        if dtype != "double":
-            raise ValueError("unsupported dtype %r for the generated path" % (dtype,))
+        if dtype in FP64_NAMES:
+            form = "double"
+        elif dtype in FP32C_NAMES:
+            form = "float32c" if model_info.raw.get("f32c") else "double"
+        else:
+            raise ValueError("unsupported dtype %r" % (dtype,))
+        self.form = form
         self.dtype = np.dtype('d')
         self.device = device
-        self.lib = _abi.load_library(model_info.id, lib_dir)
+        self.lib = _abi.load_library(model_info.id, lib_dir, form)
 
     def make_kernel(self, q_vectors, reorder=True):
         return B200Kernel(self, q_vectors, reorder=reorder)

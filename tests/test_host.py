@@ -138,8 +138,9 @@ def test_library_exports_header_symbols(name):
     path = _abi.library_path(name)
     assert os.path.exists(path), "library not built: %s" % path
     lib = ct.CDLL(path)
-    for suffix in _header_suffixes():
-        getattr(lib, "sasb200_%s_%s" % (name, suffix))
+    for prefix in (name, name + "_f32c"):
+        for suffix in _header_suffixes():
+            getattr(lib, "sasb200_%s_%s" % (prefix, suffix))
     meta = _abi.load_metadata(name)
     assert meta["id"] == name
 
