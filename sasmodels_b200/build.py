@@ -83,7 +83,8 @@ def build_model(name, force=False, verbose=False, extra_flags=()):
                               + _read(os.path.join(CSRC, "sas_device.cuh"))
                               + _read(os.path.join(CSRC, "sas_noalloc.cuh"))
                               + _read(os.path.join(CSRC, "fp32c_math.cuh"))
-                              + _read(os.path.join(CSRC, "fp32c_models.cuh")))
+                              + _read(os.path.join(CSRC, "fp32c_models.cuh"))
+                              + _read(os.path.join(CSRC, "sas_batch.cuh")))
     meta["build_tag"] = tag
     os.makedirs(LIB, exist_ok=True)
     os.makedirs(BUILD, exist_ok=True)

@@ -34,30 +34,95 @@ constexpr double PI_4 = 0.7853981633974483;     // kernel_header.c M_PI_4
 constexpr double PI = 3.141592653589793;
 constexpr double FOUR_PI_3 = 4.18879020478639;  // kernel_header.c M_4PI_3
 
-// ---- sphere ---------------------------------------------------------------
-__device__ __forceinline__ void sphere_fq(double q, double sld, double solvent,
-                                         double radius, double &F1, double &F2)
+// ---- quadrature functors ---------------------------------------------------
+// A 1D orientation/shape average is split into
+//   setup(q, v)            per (q, mesh point) constants and the Gauss rule,
+//   nodes(S)               number of rule points,
+//   node(S, i, t1, t2)     add point i's w*F and w*F^2 to FP64 sums,
+//   finish(S, t1, t2, ..)  scale to <F>, <F^2>,
+// so the same arithmetic serves one lane walking all points (quad_fq) and a
+// warp sharing the points of one (q, mesh point) in the batched kernel.
+
+template <class Q>
+__device__ __forceinline__ void quad_fq(double q, const double *v, double &F1, double &F2)
 {
-    const double bes = (double)sph_j1c_f(q*radius);
-    const double form = (sld - solvent)*(FOUR_PI_3*radius*radius*radius)*bes;
-    F1 = 1.0e-2*form;
-    F2 = 1.0e-4*form*form;
+    const typename Q::S s = Q::setup(q, v);
+    double t1 = 0.0, t2 = 0.0;
+    const int n = Q::nodes(s);
+    for (int i = 0; i < n; ++i) Q::node(s, i, t1, t2);
+    Q::finish(s, t1, t2, F1, F2);
 }
 
-// ---- core_shell_sphere ----------------------------------------------------
-__device__ __forceinline__ void core_shell_sphere_fq(double q, double radius, double thickness,
-                                                     double core_sld, double shell_sld,
-                                                     double solvent_sld, double &F1, double &F2)
-{
-    const double rt = radius + thickness;
-    const float core = (float)(FOUR_PI_3*radius*radius*radius*(core_sld - shell_sld));
-    const float shell = (float)(FOUR_PI_3*rt*rt*rt*(shell_sld - solvent_sld));
-    const float f = core*sph_j1c_f(q*radius) + shell*sph_j1c_f(q*rt);
-    F1 = 1.0e-2*(double)f;
-    F2 = 1.0e-4*(double)f*(double)f;
-}
+// sphere (sphere.c:13-20): v = sld, sld_solvent, radius; one "node"
+struct QuadSphere {
+    struct S { double q, r, s; };
+    __device__ static S setup(double q, const double *v)
+    {
+        return S{q, v[2], (v[0] - v[1])*(FOUR_PI_3*v[2]*v[2]*v[2])};
+    }
+    __device__ static int nodes(const S &) { return 1; }
+    __device__ static void node(const S &s, int, double &t1, double &t2)
+    {
+        const double f = s.s*(double)sph_j1c_f(s.q*s.r);
+        t1 += f;
+        t2 = fma(f, f, t2);
+    }
+    __device__ static void finish(const S &, double t1, double t2, double &F1, double &F2)
+    {
+        F1 = 1.0e-2*t1;
+        F2 = 1.0e-4*t2;
+    }
+};
 
-// ---- cylinder ---------------------------------------------------------------
+// core_shell_sphere (core_shell_sphere.c:19-30, lib/core_shell.c:8-30):
+// v = radius, thickness, sld_core, sld_shell, sld_solvent; one "node"
+struct QuadCoreShellSphere {
+    struct S { double q, r, rt; float core, shell; };
+    __device__ static S setup(double q, const double *v)
+    {
+        const double rt = v[0] + v[1];
+        return S{q, v[0], rt, (float)(FOUR_PI_3*v[0]*v[0]*v[0]*(v[2] - v[3])),
+                 (float)(FOUR_PI_3*rt*rt*rt*(v[3] - v[4]))};
+    }
+    __device__ static int nodes(const S &) { return 1; }
+    __device__ static void node(const S &s, int, double &t1, double &t2)
+    {
+        const double f = (double)(s.core*sph_j1c_f(s.q*s.r) + s.shell*sph_j1c_f(s.q*s.rt));
+        t1 += f;
+        t2 = fma(f, f, t2);
+    }
+    __device__ static void finish(const S &, double t1, double t2, double &F1, double &F2)
+    {
+        F1 = 1.0e-2*t1;
+        F2 = 1.0e-4*t2;
+    }
+};
+
+// cylinder (cylinder.c:55-88): v = sld, sld_solvent, radius, length, ...
+struct QuadCylinder {
+    struct S { double qr, qh, s; Rule r; };
+    __device__ static S setup(double q, const double *v)
+    {
+        const double radius = v[2], length = v[3];
+        return S{q*radius, q*0.5*length, (v[0] - v[1])*(PI*radius*radius*length),
+                 rule_for(q*fmax(radius, 0.5*length))};
+    }
+    __device__ static int nodes(const S &s) { return s.r.n; }
+    __device__ static void node(const S &s, int i, double &t1, double &t2)
+    {
+        const double st = s.r.st[i], ct = s.r.ct[i];
+        const float form = j1c_f(s.qr*st)*sinc_f(s.qh*ct);
+        const double wf = s.r.w[i]*st*(double)form;
+        t1 += wf;
+        t2 = fma(wf, (double)form, t2);
+    }
+    __device__ static void finish(const S &s, double t1, double t2, double &F1, double &F2)
+    {
+        F1 = 1.0e-2*s.s*(t1*PI_4);
+        F2 = 1.0e-4*s.s*s.s*(t2*PI_4);
+    }
+};
+
 __device__ __forceinline__ double cylinder_iqac(double qab, double qc, double sld,
                                                 double solvent, double radius, double length)
 {
@@ -67,28 +132,35 @@ __device__ __forceinline__ double cylinder_iqac(double qab, double qc, double sl
     return 1.0e-4*a*a;
 }
 
-__device__ __forceinline__ void cylinder_fq(double q, double sld, double solvent,
-                                            double radius, double length,
-                                            double &F1, double &F2)
-{
-    const Rule r = rule_for(q*fmax(radius, 0.5*length));
-    const double qr = q*radius, qh = q*0.5*length;
-    double t1 = 0.0, t2 = 0.0;
-    for (int i = 0; i < r.n; ++i) {
-        const double st = r.st[i], ct = r.ct[i];
-        const float form = j1c_f(qr*st)*sinc_f(qh*ct);
-        const double wf = r.w[i]*st*(double)form;
-        t1 += wf;
-        t2 = fma(wf, (double)form, t2);
+// ellipsoid (ellipsoid.c:50-91): v = sld, sld_solvent, radius_polar,
+// radius_equatorial, ...  The section radius Re sqrt(1 + u^2 (v^2-1)) at
+// u = cos(angle) enters as the phase q r = sqrt(A + B u^2), formed in FP64.
+struct QuadEllipsoid {
+    struct S { double A, B, s; Rule r; };
+    __device__ static S setup(double q, const double *v)
+    {
+        const double rp = v[2], re = v[3];
+        const double ratio = rp/re;
+        const double A = (q*re)*(q*re);
+        return S{A, A*(ratio*ratio - 1.0), (v[0] - v[1])*(FOUR_PI_3*rp*re*re),
+                 rule_for(q*fmax(rp, re))};
     }
-    const double s = (sld - solvent)*(PI*radius*radius*length);
-    F1 = 1.0e-2*s*(t1*PI_4);
-    F2 = 1.0e-4*s*s*(t2*PI_4);
-}
+    __device__ static int nodes(const S &s) { return s.r.n; }
+    __device__ static void node(const S &s, int i, double &t1, double &t2)
+    {
+        const double u = fma(s.r.z[i], 0.5, 0.5);
+        const double f = (double)sph_j1c_f(sqrt_d_fast(fma(s.B, u*u, s.A)));
+        const double wf = s.r.w[i]*f;
+        t1 += wf;
+        t2 = fma(wf, f, t2);
+    }
+    __device__ static void finish(const S &s, double t1, double t2, double &F1, double &F2)
+    {
+        F1 = 1.0e-2*s.s*(0.5*t1);
+        F2 = 1.0e-4*s.s*s.s*(0.5*t2);
+    }
+};
 
-// ---- ellipsoid --------------------------------------------------------------
-// Radius of the ellipse section at u = cos(angle): Re sqrt(1 + u^2 (v^2-1)),
-// v = Rp/Re; the phase q*r is formed as sqrt(A + B u^2) in FP64.
 __device__ __forceinline__ double ellipsoid_iqac(double qab, double qc, double sld,
                                                  double solvent, double rp, double re)
 {
@@ -98,46 +170,24 @@ __device__ __forceinline__ double ellipsoid_iqac(double qab, double qc, double s
     return 1.0e-4*(f*s)*(f*s);
 }
 
-__device__ __forceinline__ void ellipsoid_fq(double q, double sld, double solvent,
-                                             double rp, double re, double &F1, double &F2)
-{
-    const double ratio = rp/re;
-    const double v2m1 = ratio*ratio - 1.0;
-    const Rule r = rule_for(q*fmax(rp, re));
-    const double A = (q*re)*(q*re);
-    const double B = A*v2m1;
-    double t1 = 0.0, t2 = 0.0;
-    for (int i = 0; i < r.n; ++i) {
-        const double u = fma(r.z[i], 0.5, 0.5);
-        const double f = (double)sph_j1c_f(sqrt_d_fast(fma(B, u*u, A)));
-        const double wf = r.w[i]*f;
-        t1 += wf;
-        t2 = fma(wf, f, t2);
-    }
-    const double s = (sld - solvent)*(FOUR_PI_3*rp*re*re);
-    F1 = 1.0e-2*s*(0.5*t1);
-    F2 = 1.0e-4*s*s*(0.5*t2);
-}
-
-// ---- core_shell_cylinder ----------------------------------------------------
+// core_shell_cylinder (core_shell_cylinder.c:4-7, 60-123): v = sld_core,
+// sld_shell, sld_solvent, radius, thickness, length, ...
 struct CoreShellCyl {
     double core_r, core_h, shell_r, shell_h;
     float core_vd, shell_vd;
     double rmax;
 };
 
-__device__ __forceinline__ CoreShellCyl core_shell_cylinder_setup(
-    double core_sld, double shell_sld, double solvent_sld,
-    double radius, double thickness, double length)
+__device__ __forceinline__ CoreShellCyl core_shell_cylinder_setup(const double *v)
 {
+    const double radius = v[3], thickness = v[4], length = v[5];
     CoreShellCyl c;
     c.core_r = radius;
     c.core_h = 0.5*length;
     c.shell_r = radius + thickness;
     c.shell_h = 0.5*length + thickness;
-    c.core_vd = (float)(PI*radius*radius*length*(core_sld - shell_sld));
-    c.shell_vd = (float)(PI*c.shell_r*c.shell_r*(length + 2.0*thickness)
-                         *(shell_sld - solvent_sld));
+    c.core_vd = (float)(PI*radius*radius*length*(v[0] - v[1]));
+    c.shell_vd = (float)(PI*c.shell_r*c.shell_r*(length + 2.0*thickness)*(v[1] - v[2]));
     c.rmax = fmax(c.shell_r, c.shell_h);
     return c;
 }
@@ -149,33 +199,33 @@ __device__ __forceinline__ float core_shell_cylinder_amp(const CoreShellCyl &c,
          + c.shell_vd*sinc_f(c.shell_h*qc)*j1c_f(c.shell_r*qab);
 }
 
-__device__ __forceinline__ double core_shell_cylinder_iqac(
-    double qab, double qc, double core_sld, double shell_sld, double solvent_sld,
-    double radius, double thickness, double length)
-{
-    const CoreShellCyl c = core_shell_cylinder_setup(core_sld, shell_sld, solvent_sld,
-                                                     radius, thickness, length);
-    const double f = (double)core_shell_cylinder_amp(c, qab, qc);
-    return 1.0e-4*f*f;
-}
-
-__device__ __forceinline__ void core_shell_cylinder_fq(
-    double q, double core_sld, double shell_sld, double solvent_sld,
-    double radius, double thickness, double length, double &F1, double &F2)
-{
-    const CoreShellCyl c = core_shell_cylinder_setup(core_sld, shell_sld, solvent_sld,
-                                                     radius, thickness, length);
-    const Rule r = rule_for(q*c.rmax);
-    double t1 = 0.0, t2 = 0.0;
-    for (int i = 0; i < r.n; ++i) {
-        const double st = r.st[i], ct = r.ct[i];
-        const float f = core_shell_cylinder_amp(c, q*st, q*ct);
-        const double wf = r.w[i]*st*(double)f;
+struct QuadCoreShellCylinder {
+    struct S { double q; CoreShellCyl c; Rule r; };
+    __device__ static S setup(double q, const double *v)
+    {
+        const CoreShellCyl c = core_shell_cylinder_setup(v);
+        return S{q, c, rule_for(q*c.rmax)};
+    }
+    __device__ static int nodes(const S &s) { return s.r.n; }
+    __device__ static void node(const S &s, int i, double &t1, double &t2)
+    {
+        const double st = s.r.st[i], ct = s.r.ct[i];
+        const float f = core_shell_cylinder_amp(s.c, s.q*st, s.q*ct);
+        const double wf = s.r.w[i]*st*(double)f;
         t1 += wf;
         t2 = fma(wf, (double)f, t2);
     }
-    F1 = 1.0e-2*(t1*PI_4);
-    F2 = 1.0e-4*(t2*PI_4);
+    __device__ static void finish(const S &, double t1, double t2, double &F1, double &F2)
+    {
+        F1 = 1.0e-2*(t1*PI_4);
+        F2 = 1.0e-4*(t2*PI_4);
+    }
+};
+
+__device__ __forceinline__ double core_shell_cylinder_iqac(double qab, double qc, const double *v)
+{
+    const double f = (double)core_shell_cylinder_amp(core_shell_cylinder_setup(v), qab, qc);
+    return 1.0e-4*f*f;
 }
 
 }  // namespace f32c

@@ -32,6 +32,25 @@ def call_Fq(calculator, pars, cutoff=0., mono=False):
     return calculator.Fq(call_details, values, cutoff, is_magnetic, R_eff_type)
 
 
+class _CallShape:
+    """The attributes of a Kernel that make_kernel_args reads."""
+    def __init__(self, info, dim):
+        import numpy as np
+        self.info = info
+        self.dim = dim
+        self.dtype = np.dtype('d')
+
+
+def make_call_args(model_info, pars, q_vectors, mono=False):
+    """(call_details, values, is_magnetic) for *pars* at *q_vectors* without
+    building a kernel: the arrays a kernel call (or a batch) consumes."""
+    dim = '2d' if len(q_vectors) == 2 else '1d'
+    pars = dict(pars)
+    pars.pop(RADIUS_MODE_ID, None)
+    mesh = get_mesh(model_info, pars, dim=dim, mono=mono)
+    return make_kernel_args(_CallShape(model_info, dim), mesh)
+
+
 def get_mesh(model_info, values, dim='1d', mono=False):
     """
     One (value, dispersity, weights) tuple per call parameter; parameters not

@@ -379,6 +379,8 @@ def make_cuda_source(sm_info, sources):
     body.append("SASB200_EXPORT_MODEL(%s, sasm::SasModel)" % sm_info.id)
     if f32c:
         body.append("SASB200_EXPORT_MODEL(%s_f32c, sasm::SasModelF32c)" % sm_info.id)
+        body.append('#include "sas_batch.cuh"')
+        body.append("SASB200_EXPORT_BATCH(%s, sasm::SasModel, sasm::SasModelF32c)" % sm_info.id)
     if sm_info.id in NOALLOC_EXPORTS:
         variant, var = NOALLOC_EXPORTS[sm_info.id]
         body.append('#include "sas_noalloc.cuh"')
@@ -394,21 +396,17 @@ def make_cuda_source(sm_info, sources):
 #: models with hand-written FP32-compensated physics (csrc/fp32c_models.cuh):
 #: expected kernel parameter order and the binding of fq/iqac to it
 F32C_MODELS = {
-    "sphere": (["sld", "sld_solvent", "radius"],
-               "f32c::sphere_fq(q, v[0], v[1], v[2], F1, F2);", None),
+    "sphere": (["sld", "sld_solvent", "radius"], "QuadSphere", None),
     "core_shell_sphere": (["radius", "thickness", "sld_core", "sld_shell", "sld_solvent"],
-                          "f32c::core_shell_sphere_fq(q, v[0], v[1], v[2], v[3], v[4], F1, F2);",
-                          None),
-    "cylinder": (["sld", "sld_solvent", "radius", "length", "theta", "phi"],
-                 "f32c::cylinder_fq(q, v[0], v[1], v[2], v[3], F1, F2);",
+                          "QuadCoreShellSphere", None),
+    "cylinder": (["sld", "sld_solvent", "radius", "length", "theta", "phi"], "QuadCylinder",
                  "return f32c::cylinder_iqac(qab, qc, v[0], v[1], v[2], v[3]);"),
     "ellipsoid": (["sld", "sld_solvent", "radius_polar", "radius_equatorial", "theta", "phi"],
-                  "f32c::ellipsoid_fq(q, v[0], v[1], v[2], v[3], F1, F2);",
+                  "QuadEllipsoid",
                   "return f32c::ellipsoid_iqac(qab, qc, v[0], v[1], v[2], v[3]);"),
     "core_shell_cylinder": (["sld_core", "sld_shell", "sld_solvent", "radius", "thickness",
-                             "length", "theta", "phi"],
-                            "f32c::core_shell_cylinder_fq(q, v[0], v[1], v[2], v[3], v[4], v[5], F1, F2);",
-                            "return f32c::core_shell_cylinder_iqac(qab, qc, v[0], v[1], v[2], v[3], v[4], v[5]);"),
+                             "length", "theta", "phi"], "QuadCoreShellCylinder",
+                            "return f32c::core_shell_cylinder_iqac(qab, qc, v);"),
 }
 
 _GAUSS_RE = re.compile(r"constant\s+double\s+Gauss(\d+)(Z|Wt)\s*\[\s*\d*\s*\]\s*=\s*\{(.*?)\}", re.S)
@@ -467,7 +465,9 @@ def f32c_block(name, table, codes):
     out.append("}  // namespace f32c")
     out.append("namespace sasm {")
     out.append("struct SasModelF32c : SasModel {")
-    out.append("  __device__ static void fq(double q, double &F1, double &F2, const double *v) { %s }" % fq)
+    out.append("  using Quad = f32c::%s;" % fq)
+    out.append("  __device__ static void fq(double q, double &F1, double &F2, const double *v)"
+               " { f32c::quad_fq<Quad>(q, v, F1, F2); }")
     out.append("  __device__ static double iq(double q, const double *v) { double F1, F2; fq(q, F1, F2, v); return F2; }")
     if iqac:
         out.append("  __device__ static double iqac(double qab, double qc, const double *v) { %s }" % iqac)
