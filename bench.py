@@ -245,6 +245,11 @@ def run_b200(args, world, rank, local):
     stream = kernel.stream
     launches_per_step = 3   # mesh_prepare, iq_main, finalize
 
+    tile = 0
+    if not args.no_tune:
+        from sasmodels_b200 import autotune
+        tile = autotune.tune_kernel(kernel, variant, dev_d, dev_v, n_mesh, reps=1,
+                                    budget_s=15.0)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             kernel.launch(variant, dev_d, dev_v, 0, n_mesh, 0.0, 0)
@@ -304,6 +309,7 @@ def run_b200(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": desc, "evals_per_step": evals, "nq": nq,
+                       "tile": "0x%08x (autotuned)" % tile if tile else "library default",
                        "mesh": n_mesh, "l2": "flushed (256 MB write) before each timed step",
                        "parallelism": "replicas x%d (one workload per GPU)" % world},
             "e2e": e2e,
@@ -319,12 +325,114 @@ def run_b200(args, world, rank, local):
         s = clocks.summary()
         if s:
             line["clocks"] = s
+        if world == 1 and not args.no_extras and args.config == "cylinder2d":
+            line["extra"] = extras(dev)
         if world == 1 and not args.no_cpu:
             v, threads, sample, _, _ = cpu_baseline(args.config)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads,
                                     "kind": "reference", "sample": sample}
         print(json.dumps(line), flush=True)
     return line
+
+
+def time_launches(kernel, variant, dd, dv, n_mesh, reps):
+    import torch
+    stream = kernel.stream
+    with torch.cuda.stream(stream):
+        kernel.launch(variant, dd, dv, 0, n_mesh, 0.0, 0)
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(reps):
+            kernel.launch(variant, dd, dv, 0, n_mesh, 0.0, 0)
+        stop.record(stream)
+    stop.synchronize()
+    return start.elapsed_time(stop)*1e-3/reps
+
+
+def single_config(name, qv, pars, dtype, reps, dev):
+    """evals/s of one plain call shape (inputs resident)."""
+    from sasmodels_b200 import load_model
+    model = load_model(name, dtype=dtype, device=dev)
+    kernel = model.make_kernel(qv)
+    details, values, magnetic = marshal(model.info, pars, qv)
+    dd, dv = kernel.upload(details, values)
+    t = time_launches(kernel, kernel.variant(magnetic), dd, dv, details.num_eval, reps)
+    return len(qv[0])*details.num_eval/t, t
+
+
+def population_compare(n_sets, stride, dev):
+    """Batched FP32c vs plain FP64 per-set launches on every `stride`-th set
+    of the seeded population: param-sets/s of both and the max relative
+    error of the batched I(q) against the FP64 plain results."""
+    import torch
+    from sasmodels_b200 import autotune, load_model, workloads
+    from sasmodels_b200.batch import Population
+    pop = workloads.population(n_sets=n_sets, seed=1)[::stride]
+    by = {}
+    for k, (name, q, pars) in enumerate(pop):
+        by.setdefault(name, []).append((k, q, pars))
+    t_batch = t_plain = 0.0
+    worst = 0.0
+    tuned = {}
+    for name, members in by.items():
+        sets = [(q, p) for _, q, p in members]
+        warps, ipw = autotune.tune_population(name, sets, "float32c")
+        tuned[name] = [warps, ipw]
+        P = Population(name, sets, form="float32c", device=dev, warps=warps,
+                       items_per_warp=ipw)
+        P.run()
+        P.stream.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record(P.stream)
+        P.run()
+        stop.record(P.stream)
+        stop.synchronize()
+        t_batch += start.elapsed_time(stop)*1e-3
+        iq_batch = P.iq()
+        model = load_model(name, device=dev)
+        calls = []
+        for q, pars in sets:
+            k = model.make_kernel([q])
+            d, v, _ = marshal(model.info, pars, [q])
+            dd, dv = k.upload(d, v)
+            calls.append((k, dd, dv, d.num_eval, v))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k, dd, dv, n, _ in calls:
+            with torch.cuda.stream(k.stream):
+                k.launch("Iq", dd, dv, 0, n, 0.0, 0)
+            k.stream.synchronize()
+        t_plain += time.perf_counter() - t0
+        for (k, dd, dv, n, v), iq_b in zip(calls, iq_batch):
+            raw = k._result_dev.cpu().numpy()
+            nq = k.q_input.nq
+            total = raw[2*nq] or 1.0
+            shell = raw[2*nq + 2]/total or 1.0
+            iq64 = v[0]/shell*raw[0:2*nq:2]/total + v[1]
+            worst = max(worst, float(np.max(np.abs(iq_b - iq64)/np.abs(iq64))))
+    n = len(pop)
+    return {"sets": n, "sample": "every %d-th of %d seeded sets" % (stride, n_sets),
+            "batched_f32c_sets_per_s": n/t_batch, "plain_f64_sets_per_s": n/t_plain,
+            "speedup": t_plain/t_batch, "max_rel_err_vs_f64": worst,
+            "autotuned": tuned}
+
+
+def extras(dev):
+    """Secondary measurements of the other headline configurations."""
+    from sasmodels_b200 import workloads
+    out = {}
+    name, qv, pars = workloads.sphere_1d()
+    v, t = single_config(name, qv, pars, "double", 200, dev)
+    out["sphere1d_f64"] = {"evals_per_s": v, "ms_per_call": 1e3*t}
+    name, qv, pars = workloads.core_shell_sphere_magnetic()
+    for dtype in ("double", "float32c"):
+        v, t = single_config(name, qv, pars, dtype, 20, dev)
+        out["magnetic_" + dtype] = {"evals_per_s": v, "ms_per_call": 1e3*t,
+                                    "spin_channels": 6}
+    out["population"] = population_compare(4096, 8, dev)
+    return out
 
 
 #: FP64 flops issued per evaluation of each workload's dominant kernel,
@@ -350,6 +458,9 @@ def main(argv=None):
                     help="q grid edge for cylinder2d (smaller for profiling)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the secondary configurations")
     args = ap.parse_args(argv)
     world, rank, local = dist_setup(args.gpus)
     try:
