@@ -431,7 +431,7 @@ def extras(dev):
         v, t = single_config(name, qv, pars, dtype, 20, dev)
         out["magnetic_" + dtype] = {"evals_per_s": v, "ms_per_call": 1e3*t,
                                     "spin_channels": 6}
-    out["population"] = population_compare(4096, 8, dev)
+    out["population"] = population_compare(4096, 7, dev)
     return out
 
 

@@ -110,13 +110,14 @@ def build_model(name, force=False, verbose=False, extra_flags=()):
     return so
 
 
-def build_plain(cu_name, so_name, force=False, extra_flags=()):
+def build_plain(cu_name, so_name, force=False, extra_flags=(), extra_deps=()):
     """Compile a model-independent .cu from csrc/ into lib/ (rebuilt when the
-    source or flags change)."""
+    source, its headers or the flags change)."""
     src = os.path.join(CSRC, cu_name)
     so = os.path.join(LIB, so_name)
     flags = nvcc_flags(extra_flags)
-    tag = generate.source_tag(_read(src) + " ".join(flags))
+    tag = generate.source_tag(_read(src) + " ".join(flags)
+                              + "".join(_read(os.path.join(CSRC, d)) for d in extra_deps))
     stamp = so + ".tag"
     if not force and os.path.exists(so) and os.path.exists(stamp) and _read(stamp) == tag:
         return so
@@ -133,7 +134,9 @@ def build_plain(cu_name, so_name, force=False, extra_flags=()):
 
 def build_support(force=False):
     """Libraries that do not depend on a model plugin."""
-    return [build_plain("peaks.cu", "libsasb200_peaks.so", force)]
+    return [build_plain("peaks.cu", "libsasb200_peaks.so", force),
+            build_plain("mlp.cu", "libsasb200_mlp.so", force,
+                        extra_deps=("tc_ptx.cuh",))]
 
 
 def _read(path):

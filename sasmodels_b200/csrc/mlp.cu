@@ -1,0 +1,627 @@
+// Tensor-core MLP for the I(q) surrogate: 16 (7 used) -> 256 -> 256 -> 256
+// -> 256 -> 1, SiLU, BF16 weights and activations, FP32 accumulation in TMEM
+// (tcgen05.mma kind::f16, M = 128 rows per CTA, N = 256, K = 16 per MMA).
+//
+// Kernels
+//   mlp_forward    all four hidden layers of 128 samples per CTA; the
+//                  activations stay in shared memory as the next layer's A
+//                  operand, weights stream through a 256 x 64 staging tile;
+//                  bias + SiLU in the TMEM epilogue, the 256 -> 1 output layer
+//                  as a per-row dot product in the last epilogue.  Optionally
+//                  saves the pre-activations z and activations h for training.
+//   mlp_backward   dZ3 = dout w_out * silu'(z3), then dZ(l-1) = (dZl W_l) *
+//                  silu'(z(l-1)) through the three 256x256 layers, the same
+//                  way (A = dZ in smem, B = W_l^T streamed).
+//   gemm_nt        C_split = A[M x K] B[N x K]^T over a K range (split-K):
+//                  weight gradients dW = dZ^T H with the batch as K.
+//   + transpose, row sums/dots, MSE gradient, Adam, feature packing.
+//
+// All launches return an error code; device-side waits are bounded and
+// report through *err (0 = ok).
+#include <cstdint>
+#include <cstdio>
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+#include "tc_ptx.cuh"
+
+namespace mlp {
+
+constexpr int HID = 256;
+constexpr int NIN = 16;           // padded input features
+constexpr int TM = 128;           // rows per CTA
+constexpr int KC = 64;            // streamed K chunk
+constexpr int THREADS = 128;
+constexpr int FWD_SMEM = TM*HID*2 + HID*KC*2;      // 64 KB act + 32 KB weights
+constexpr int GEMM_SMEM = 100*1024;                // keeps <= 2 CTAs per SM (TMEM)
+
+struct Weights {
+    const __nv_bfloat16 *w[4];    // w[0]: 256 x 16, w[1..3]: 256 x 256, [out][in]
+    const float *b[4];
+    const float *w_out;
+    const float *b_out;           // device scalar
+};
+
+__device__ __forceinline__ float silu(float z) { return z/(1.0f + __expf(-z)); }
+__device__ __forceinline__ float dsilu(float z)
+{
+    const float s = 1.0f/(1.0f + __expf(-z));
+    return s*(1.0f + z*(1.0f - s));
+}
+
+__device__ __forceinline__ uint32_t pack2(float a, float b)
+{
+    __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t *>(&v);
+}
+
+__device__ __forceinline__ float bf_lo(uint32_t u) { return __uint_as_float(u << 16); }
+__device__ __forceinline__ float bf_hi(uint32_t u) { return __uint_as_float(u & 0xffff0000u); }
+
+// Copy a ROWS x K (K-major, row stride ld elements) bf16 block starting at
+// column k0 into a canonical K-major smem tile; rows >= nrows read as zero.
+template <int ROWS, int K>
+__device__ __forceinline__ void load_tile(uint8_t *tile, const __nv_bfloat16 *src, int ld,
+                                          int k0, int nrows)
+{
+    constexpr int VEC = ROWS*(K/8);
+    for (int i = threadIdx.x; i < VEC; i += THREADS) {
+        const int r = i/(K/8), c = i % (K/8);
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (r < nrows)
+            v = *reinterpret_cast<const uint4 *>(src + (size_t)r*ld + k0 + 8*c);
+        *reinterpret_cast<uint4 *>(tile + tc::kmajor_offset<ROWS>(r, 8*c)) = v;
+    }
+}
+
+struct Pipe {
+    uint64_t *bar;
+    uint32_t phase;
+    bool ok;
+};
+
+// Issue the MMAs of one staged chunk (single thread), then wait (all).
+// a_addr: canonical 128-row A tile holding the full K; a_step0: first K=16
+// step of this chunk within A; b_addr: canonical NB-row tile of this chunk.
+template <int NB, int STEPS>
+__device__ __forceinline__ void mma_chunk(Pipe &pp, uint32_t tmem, uint32_t a_addr, int a_step0,
+                                          uint32_t b_addr, bool accumulate)
+{
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (threadIdx.x == 0) {
+        constexpr uint32_t idesc = tc::idesc_bf16(128, NB);
+        #pragma unroll
+        for (int s = 0; s < STEPS; ++s) {
+            tc::mma_bf16(tmem, tc::kmajor_desc<128>(a_addr, a_step0 + s),
+                         tc::kmajor_desc<NB>(b_addr, s), idesc,
+                         (accumulate || s > 0) ? 1u : 0u);
+        }
+        tc::mma_commit(pp.bar);
+    }
+    const bool done = tc::mbar_wait(pp.bar, pp.phase);
+    pp.phase ^= 1u;
+    pp.ok = __syncthreads_and(done && pp.ok) != 0;
+    tc::fence_after_sync();
+}
+
+// A (128 x 256, resident) times a streamed [256 x 256] weight (rows = N).
+__device__ __forceinline__ void layer_256(Pipe &pp, uint32_t tmem, uint8_t *act, uint8_t *wbuf,
+                                          const __nv_bfloat16 *w)
+{
+    const uint32_t a_addr = tc::smem_u32(act), b_addr = tc::smem_u32(wbuf);
+    for (int kc = 0; kc < HID/KC; ++kc) {
+        if (!pp.ok) return;
+        load_tile<HID, KC>(wbuf, w, HID, kc*KC, HID);
+        mma_chunk<HID, KC/16>(pp, tmem, a_addr, kc*(KC/16), b_addr, kc > 0);
+    }
+}
+
+// Read this thread's TMEM row (cols c0..c0+15) into floats.
+__device__ __forceinline__ void tmem_row16(uint32_t tmem, int c0, float (&v)[16])
+{
+    uint32_t r[16];
+    const uint32_t lane_base = (uint32_t)((threadIdx.x & ~31) << 16);
+    tc::tmem_ld16(tmem + lane_base + (uint32_t)c0, r);
+    tc::tmem_wait_ld();
+    #pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ void store16(uint8_t *act, int row, int c0, const float (&h)[16])
+{
+    uint4 lo, hi;
+    lo.x = pack2(h[0], h[1]);   lo.y = pack2(h[2], h[3]);
+    lo.z = pack2(h[4], h[5]);   lo.w = pack2(h[6], h[7]);
+    hi.x = pack2(h[8], h[9]);   hi.y = pack2(h[10], h[11]);
+    hi.z = pack2(h[12], h[13]); hi.w = pack2(h[14], h[15]);
+    *reinterpret_cast<uint4 *>(act + tc::kmajor_offset<TM>(row, c0)) = lo;
+    *reinterpret_cast<uint4 *>(act + tc::kmajor_offset<TM>(row, c0 + 8)) = hi;
+}
+
+__device__ __forceinline__ void save16(__nv_bfloat16 *dst, const float (&h)[16])
+{
+    uint4 lo, hi;
+    lo.x = pack2(h[0], h[1]);   lo.y = pack2(h[2], h[3]);
+    lo.z = pack2(h[4], h[5]);   lo.w = pack2(h[6], h[7]);
+    hi.x = pack2(h[8], h[9]);   hi.y = pack2(h[10], h[11]);
+    hi.z = pack2(h[12], h[13]); hi.w = pack2(h[14], h[15]);
+    reinterpret_cast<uint4 *>(dst)[0] = lo;
+    reinterpret_cast<uint4 *>(dst)[1] = hi;
+}
+
+__device__ __forceinline__ void load16(const __nv_bfloat16 *src, float (&z)[16])
+{
+    const uint4 lo = reinterpret_cast<const uint4 *>(src)[0];
+    const uint4 hi = reinterpret_cast<const uint4 *>(src)[1];
+    const uint32_t u[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+    #pragma unroll
+    for (int j = 0; j < 8; ++j) { z[2*j] = bf_lo(u[j]); z[2*j + 1] = bf_hi(u[j]); }
+}
+
+// Epilogue of hidden layer l: z = acc + b, h = silu(z); h back into the
+// activation tile (next A), z and h optionally to global; the last layer
+// also forms out = h . w_out + b_out.
+__device__ __forceinline__ void epilogue_hidden(uint32_t tmem, uint8_t *act, const float *bias,
+                                                const float *w_out, const float *b_out, bool last,
+                                                int grow, int n, __nv_bfloat16 *zs,
+                                                __nv_bfloat16 *hs, float *out)
+{
+    const int t = threadIdx.x;
+    float dot = 0.0f;
+    for (int c0 = 0; c0 < HID; c0 += 16) {
+        float z[16], h[16];
+        tmem_row16(tmem, c0, z);
+        #pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            z[j] += bias[c0 + j];
+            h[j] = silu(z[j]);
+        }
+        if (last) {
+            #pragma unroll
+            for (int j = 0; j < 16; ++j) dot = fmaf(h[j], w_out[c0 + j], dot);
+        } else {
+            store16(act, t, c0, h);
+        }
+        if (zs != nullptr) {          // every row of the padded batch (zero inputs)
+            save16(zs + (size_t)grow*HID + c0, z);
+            save16(hs + (size_t)grow*HID + c0, h);
+        }
+    }
+    if (last && grow < n) out[grow] = dot + *b_out;
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+mlp_forward(int n, const __nv_bfloat16 *__restrict__ x, Weights wts, float *__restrict__ out,
+            __nv_bfloat16 *__restrict__ z_save, __nv_bfloat16 *__restrict__ h_save,
+            int *__restrict__ err)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *act = smem;
+    uint8_t *wbuf = smem + TM*HID*2;
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_slot;
+    const int t = threadIdx.x;
+    const int row0 = blockIdx.x*TM;
+
+    if (t < 32) {
+        tc::tmem_alloc(&tmem_slot, HID);
+        tc::tmem_relinquish();
+    }
+    if (t == 0) {
+        tc::mbar_init(&bar, 1);
+        tc::mbar_fence_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+    Pipe pp{&bar, 0u, true};
+
+    // layer 0: K = 16 (7 features + zero padding)
+    load_tile<TM, NIN>(act, x + (size_t)row0*NIN, NIN, 0, n - row0);
+    load_tile<HID, NIN>(wbuf, wts.w[0], NIN, 0, HID);
+    mma_chunk<HID, 1>(pp, tmem, tc::smem_u32(act), 0, tc::smem_u32(wbuf), false);
+    const size_t plane = (size_t)gridDim.x*TM*HID;
+    for (int l = 0; l < 4 && pp.ok; ++l) {
+        if (l > 0) layer_256(pp, tmem, act, wbuf, wts.w[l]);
+        if (!pp.ok) break;
+        epilogue_hidden(tmem, act, wts.b[l], wts.w_out, wts.b_out, l == 3, row0 + t, n,
+                        z_save ? z_save + l*plane : nullptr,
+                        h_save ? h_save + l*plane : nullptr, out);
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (t < 32) tc::tmem_dealloc(tmem, HID);
+    if (!pp.ok && t == 0) atomicExch(err, 1);
+}
+
+// Backward through the hidden layers of 128 samples.  wt[l] = W_l^T stored
+// [in][out] (K-major B for dH = dZ W).  dz_save[l] receives dZ_l.
+struct WeightsT {
+    const __nv_bfloat16 *wt[4];   // wt[1..3] used
+    const float *w_out;
+};
+
+__global__ void __launch_bounds__(THREADS, 1)
+mlp_backward(int n, WeightsT wts, const float *__restrict__ dout,
+             const __nv_bfloat16 *__restrict__ z_save, __nv_bfloat16 *__restrict__ dz_save,
+             int *__restrict__ err)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *act = smem;
+    uint8_t *wbuf = smem + TM*HID*2;
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_slot;
+    const int t = threadIdx.x;
+    const int row0 = blockIdx.x*TM;
+    const int grow = row0 + t;
+    const size_t plane = (size_t)gridDim.x*TM*HID;
+
+    if (t < 32) {
+        tc::tmem_alloc(&tmem_slot, HID);
+        tc::tmem_relinquish();
+    }
+    if (t == 0) {
+        tc::mbar_init(&bar, 1);
+        tc::mbar_fence_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+    Pipe pp{&bar, 0u, true};
+
+    // dZ3 = dout * w_out * silu'(z3)
+    {
+        const float d = grow < n ? dout[grow] : 0.0f;
+        const __nv_bfloat16 *zrow = z_save + 3*plane + (size_t)grow*HID;
+        __nv_bfloat16 *drow = dz_save + 3*plane + (size_t)grow*HID;
+        for (int c0 = 0; c0 < HID; c0 += 16) {
+            float z[16], g[16];
+            load16(zrow + c0, z);
+            #pragma unroll
+            for (int j = 0; j < 16; ++j) g[j] = d*wts.w_out[c0 + j]*dsilu(z[j]);
+            store16(act, t, c0, g);
+            save16(drow + c0, g);
+        }
+    }
+    for (int l = 3; l >= 1 && pp.ok; --l) {
+        layer_256(pp, tmem, act, wbuf, wts.wt[l]);
+        if (!pp.ok) break;
+        const __nv_bfloat16 *zrow = z_save + (l - 1)*plane + (size_t)grow*HID;
+        __nv_bfloat16 *drow = dz_save + (l - 1)*plane + (size_t)grow*HID;
+        for (int c0 = 0; c0 < HID; c0 += 16) {
+            float g[16], z[16];
+            tmem_row16(tmem, c0, g);
+            load16(zrow + c0, z);
+            #pragma unroll
+            for (int j = 0; j < 16; ++j) g[j] *= dsilu(z[j]);
+            store16(act, t, c0, g);
+            save16(drow + c0, g);
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (t < 32) tc::tmem_dealloc(tmem, HID);
+    if (!pp.ok && t == 0) atomicExch(err, 1);
+}
+
+// C[split][M x NB] = A[M x K] B[NB x K]^T restricted to this split's K range
+// (multiples of 64).  grid = (M/128, splits).
+template <int NB>
+__global__ void __launch_bounds__(THREADS, 1)
+gemm_nt(int K, int lda, int ldb, const __nv_bfloat16 *__restrict__ A,
+        const __nv_bfloat16 *__restrict__ B, int k_per_split, float *__restrict__ C,
+        int M, int *__restrict__ err)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *abuf = smem;
+    uint8_t *bbuf = smem + TM*KC*2;
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_slot;
+    constexpr uint32_t NCOL = NB < 32 ? 32 : NB;
+    const int t = threadIdx.x;
+    const int m0 = blockIdx.x*TM;
+    const int k_begin = blockIdx.y*k_per_split;
+    const int k_end = min(K, k_begin + k_per_split);
+
+    if (t < 32) {
+        tc::tmem_alloc(&tmem_slot, NCOL);
+        tc::tmem_relinquish();
+    }
+    if (t == 0) {
+        tc::mbar_init(&bar, 1);
+        tc::mbar_fence_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+    Pipe pp{&bar, 0u, true};
+    bool any = false;
+    for (int k0 = k_begin; k0 < k_end && pp.ok; k0 += KC) {
+        load_tile<TM, KC>(abuf, A + (size_t)m0*lda, lda, k0, M - m0);
+        load_tile<NB, KC>(bbuf, B, ldb, k0, NB);
+        mma_chunk<NB, KC/16>(pp, tmem, tc::smem_u32(abuf), 0, tc::smem_u32(bbuf), any);
+        any = true;
+    }
+    if (pp.ok) {
+        float *crow = C + ((size_t)blockIdx.y*M + m0 + t)*NB;
+        const bool valid = m0 + t < M;
+        for (int c0 = 0; c0 < NB; c0 += 16) {
+            float v[16];
+            tmem_row16(tmem, c0, v);
+            if (!any) {
+                #pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] = 0.0f;
+            }
+            if (valid) {
+                #pragma unroll
+                for (int j = 0; j < 16; j += 4)
+                    *reinterpret_cast<float4 *>(crow + c0 + j) = make_float4(v[j], v[j+1], v[j+2], v[j+3]);
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (t < 32) tc::tmem_dealloc(tmem, NCOL);
+    if (!pp.ok && t == 0) atomicExch(err, 1);
+}
+
+// ---- small CUDA-core kernels ------------------------------------------------
+
+// dst[c][r] = src[r][c]  (bf16), 32x32 tiles through shared memory
+__global__ void transpose_bf16(int rows, int cols, const __nv_bfloat16 *__restrict__ src,
+                               __nv_bfloat16 *__restrict__ dst)
+{
+    __shared__ __nv_bfloat16 tile[32][33];
+    const int bx = blockIdx.x*32, by = blockIdx.y*32;
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int r = by + j, c = bx + threadIdx.x;
+        if (r < rows && c < cols) tile[j][threadIdx.x] = src[(size_t)r*cols + c];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int c = bx + j, r = by + threadIdx.x;
+        if (r < rows && c < cols) dst[(size_t)c*rows + r] = tile[threadIdx.x][j];
+    }
+}
+
+// out[r] = sum_c M[r][c] * (v ? v[c] : 1), one warp per row, fixed order
+__global__ void row_dot(int rows, int cols, const __nv_bfloat16 *__restrict__ M,
+                        const float *__restrict__ v, float *__restrict__ out)
+{
+    const int r = blockIdx.x*(blockDim.x/32) + threadIdx.x/32;
+    const int lane = threadIdx.x & 31;
+    if (r >= rows) return;
+    float s = 0.0f;
+    for (int c = lane; c < cols; c += 32)
+        s = fmaf(__bfloat162float(M[(size_t)r*cols + c]), v ? v[c] : 1.0f, s);
+    #pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) out[r] = s;
+}
+
+// dout = 2 (out - y) / n on the first n rows, 0 on padding; loss partials
+__global__ void mse_grad(int n, int n_pad, const float *__restrict__ out,
+                         const float *__restrict__ y, float *__restrict__ dout,
+                         float *__restrict__ sq)
+{
+    const int i = blockIdx.x*blockDim.x + threadIdx.x;
+    if (i >= n_pad) return;
+    const float d = i < n ? out[i] - y[i] : 0.0f;
+    dout[i] = i < n ? 2.0f*d/(float)n : 0.0f;
+    sq[i] = d*d;
+}
+
+// Adam on one FP32 master tensor; grad = sum of `splits` partial gradients.
+// Writes the BF16 copy (and its transpose if wt != nullptr, rows x cols).
+__global__ void adam_step(int size, int splits, const float *__restrict__ grad, float *__restrict__ p,
+                          float *__restrict__ m, float *__restrict__ v, float lr, float b1,
+                          float b2, float eps, float bc1, float bc2, __nv_bfloat16 *__restrict__ w,
+                          __nv_bfloat16 *__restrict__ wt, int rows, int cols)
+{
+    const int i = blockIdx.x*blockDim.x + threadIdx.x;
+    if (i >= size) return;
+    float g = 0.0f;
+    for (int s = 0; s < splits; ++s) g += grad[(size_t)s*size + i];
+    const float mi = b1*m[i] + (1.0f - b1)*g;
+    const float vi = b2*v[i] + (1.0f - b2)*g*g;
+    m[i] = mi;
+    v[i] = vi;
+    const float pi = p[i] - lr*(mi/bc1)/(sqrtf(vi/bc2) + eps);
+    p[i] = pi;
+    if (w) w[i] = __float2bfloat16_rn(pi);
+    if (wt) {
+        const int r = i/cols, c = i % cols;
+        wt[(size_t)c*rows + r] = __float2bfloat16_rn(pi);
+    }
+}
+
+// Surrogate input features (7 used of 16), each mapped to [-1, 1]:
+//   log R on [log 10, log 300], log L on [log 20, log 3000], R_pd and L_pd on
+//   [0, 0.3], contrast on [-5, 5], log q on [log 1e-3, log 0.5], flag {0, 1}.
+__global__ void features(int n, int n_pad, const double *__restrict__ radius,
+                         const double *__restrict__ length, const double *__restrict__ rpd,
+                         const double *__restrict__ lpd, const double *__restrict__ drho,
+                         const double *__restrict__ q, const double *__restrict__ flag,
+                         __nv_bfloat16 *__restrict__ x)
+{
+    const int i = blockIdx.x*blockDim.x + threadIdx.x;
+    if (i >= n_pad) return;
+    float f[16];
+    #pragma unroll
+    for (int j = 0; j < 16; ++j) f[j] = 0.0f;
+    if (i < n) {
+        f[0] = (float)(2.0*(log(radius[i]) - log(10.0))/(log(300.0) - log(10.0)) - 1.0);
+        f[1] = (float)(2.0*(log(length[i]) - log(20.0))/(log(3000.0) - log(20.0)) - 1.0);
+        f[2] = (float)(2.0*rpd[i]/0.3 - 1.0);
+        f[3] = (float)(2.0*lpd[i]/0.3 - 1.0);
+        f[4] = (float)(drho[i]/5.0);
+        f[5] = (float)(2.0*(log(q[i]) - log(1e-3))/(log(0.5) - log(1e-3)) - 1.0);
+        f[6] = (float)(2.0*flag[i] - 1.0);
+    }
+    uint4 *dst = reinterpret_cast<uint4 *>(x + (size_t)i*NIN);
+    dst[0] = make_uint4(pack2(f[0], f[1]), pack2(f[2], f[3]), pack2(f[4], f[5]), pack2(f[6], f[7]));
+    dst[1] = make_uint4(pack2(f[8], f[9]), pack2(f[10], f[11]), pack2(f[12], f[13]), pack2(f[14], f[15]));
+}
+
+inline char *errbuf()
+{
+    static thread_local char buf[256] = "";
+    return buf;
+}
+
+inline int32_t status(const char *what)
+{
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        std::snprintf(errbuf(), 256, "%s: %s", what, cudaGetErrorString(e));
+        return -3;
+    }
+    return 0;
+}
+
+}  // namespace mlp
+
+using namespace mlp;
+
+extern "C" {
+
+const char *sasb200_mlp_last_error(void) { return errbuf(); }
+
+// out[n] (and z/h planes [4][n_pad x 256] when non-null) for x[n_pad x 16];
+// n_pad a multiple of 128.
+int32_t sasb200_mlp_forward(int32_t n, int32_t n_pad, const void *x, const void *const *w,
+                            const float *const *b, const float *w_out, const float *b_out, float *out,
+                            void *z_save, void *h_save, int32_t *err, void *stream)
+{
+    errbuf()[0] = 0;
+    if (n < 0 || n_pad % TM || n > n_pad || !x || !w || !b || !w_out || !b_out || !out || !err)
+        return (std::snprintf(errbuf(), 256, "bad arguments"), -1);
+    if ((z_save == nullptr) != (h_save == nullptr))
+        return (std::snprintf(errbuf(), 256, "z_save and h_save go together"), -1);
+    if (n_pad == 0) return 0;
+    Weights wts;
+    for (int l = 0; l < 4; ++l) {
+        wts.w[l] = static_cast<const __nv_bfloat16 *>(w[l]);
+        wts.b[l] = b[l];
+    }
+    wts.w_out = w_out;
+    wts.b_out = b_out;
+    cudaFuncSetAttribute(mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM);
+    mlp_forward<<<n_pad/TM, THREADS, FWD_SMEM, (cudaStream_t)stream>>>(
+        n, static_cast<const __nv_bfloat16 *>(x), wts, out,
+        static_cast<__nv_bfloat16 *>(z_save), static_cast<__nv_bfloat16 *>(h_save), err);
+    return status("mlp_forward");
+}
+
+int32_t sasb200_mlp_backward(int32_t n, int32_t n_pad, const void *const *wt, const float *w_out,
+                             const float *dout, const void *z_save, void *dz_save,
+                             int32_t *err, void *stream)
+{
+    errbuf()[0] = 0;
+    if (n < 0 || n_pad % TM || n > n_pad || !wt || !w_out || !dout || !z_save || !dz_save || !err)
+        return (std::snprintf(errbuf(), 256, "bad arguments"), -1);
+    if (n_pad == 0) return 0;
+    WeightsT wts;
+    for (int l = 0; l < 4; ++l) wts.wt[l] = static_cast<const __nv_bfloat16 *>(wt[l]);
+    wts.w_out = w_out;
+    cudaFuncSetAttribute(mlp_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM);
+    mlp_backward<<<n_pad/TM, THREADS, FWD_SMEM, (cudaStream_t)stream>>>(
+        n, wts, dout, static_cast<const __nv_bfloat16 *>(z_save),
+        static_cast<__nv_bfloat16 *>(dz_save), err);
+    return status("mlp_backward");
+}
+
+// C[splits][M x nb] partial products of A[M x K] (row stride lda) and
+// B[nb x K] (row stride ldb); M % 128 == 0, K % 64 == 0, nb in {16, 256}.
+int32_t sasb200_gemm_nt(int32_t M, int32_t nb, int32_t K, int32_t lda, int32_t ldb,
+                        const void *A, const void *B, int32_t splits, float *C, int32_t *err,
+                        void *stream)
+{
+    errbuf()[0] = 0;
+    if (M <= 0 || M % TM || K <= 0 || K % KC || splits <= 0 || !A || !B || !C || !err
+        || lda < K || ldb < K || lda % 8 || ldb % 8)
+        return (std::snprintf(errbuf(), 256, "bad arguments"), -1);
+    int per = (K + splits - 1)/splits;
+    per = ((per + KC - 1)/KC)*KC;
+    dim3 grid(M/TM, splits);
+    const __nv_bfloat16 *a = static_cast<const __nv_bfloat16 *>(A);
+    const __nv_bfloat16 *bb = static_cast<const __nv_bfloat16 *>(B);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (nb == 256) {
+        cudaFuncSetAttribute(gemm_nt<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
+        gemm_nt<256><<<grid, THREADS, GEMM_SMEM, st>>>(K, lda, ldb, a, bb, per, C, M, err);
+    } else if (nb == 16) {
+        cudaFuncSetAttribute(gemm_nt<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM);
+        gemm_nt<16><<<grid, THREADS, GEMM_SMEM, st>>>(K, lda, ldb, a, bb, per, C, M, err);
+    } else {
+        return (std::snprintf(errbuf(), 256, "nb must be 16 or 256"), -1);
+    }
+    return status("gemm_nt");
+}
+
+int32_t sasb200_transpose_bf16(int32_t rows, int32_t cols, const void *src, void *dst, void *stream)
+{
+    if (rows < 0 || cols < 0 || !src || !dst) return -1;
+    if (!rows || !cols) return 0;
+    dim3 grid((cols + 31)/32, (rows + 31)/32), block(32, 8);
+    transpose_bf16<<<grid, block, 0, (cudaStream_t)stream>>>(
+        rows, cols, static_cast<const __nv_bfloat16 *>(src), static_cast<__nv_bfloat16 *>(dst));
+    return status("transpose_bf16");
+}
+
+int32_t sasb200_row_dot(int32_t rows, int32_t cols, const void *M, const float *v, float *out,
+                        void *stream)
+{
+    if (rows < 0 || cols < 0 || !M || !out) return -1;
+    if (!rows) return 0;
+    row_dot<<<(rows + 7)/8, 256, 0, (cudaStream_t)stream>>>(
+        rows, cols, static_cast<const __nv_bfloat16 *>(M), v, out);
+    return status("row_dot");
+}
+
+int32_t sasb200_mse_grad(int32_t n, int32_t n_pad, const float *out, const float *y, float *dout,
+                         float *sq, void *stream)
+{
+    if (n < 0 || n > n_pad || !out || !y || !dout || !sq) return -1;
+    if (!n_pad) return 0;
+    mse_grad<<<(n_pad + 255)/256, 256, 0, (cudaStream_t)stream>>>(n, n_pad, out, y, dout, sq);
+    return status("mse_grad");
+}
+
+int32_t sasb200_adam(int32_t size, int32_t splits, const float *grad, float *p, float *m, float *v,
+                     float lr, float b1, float b2, float eps, int32_t step, void *w, void *wt,
+                     int32_t rows, int32_t cols, void *stream)
+{
+    if (size <= 0 || splits <= 0 || !grad || !p || !m || !v || step < 1) return -1;
+    if (wt && rows*cols != size) return -1;
+    const float bc1 = 1.0f - powf(b1, (float)step), bc2 = 1.0f - powf(b2, (float)step);
+    adam_step<<<(size + 255)/256, 256, 0, (cudaStream_t)stream>>>(
+        size, splits, grad, p, m, v, lr, b1, b2, eps, bc1, bc2,
+        static_cast<__nv_bfloat16 *>(w), static_cast<__nv_bfloat16 *>(wt), rows, cols);
+    return status("adam_step");
+}
+
+int32_t sasb200_mlp_features(int32_t n, int32_t n_pad, const double *radius, const double *length,
+                             const double *rpd, const double *lpd, const double *drho,
+                             const double *q, const double *flag, void *x, void *stream)
+{
+    if (n < 0 || n > n_pad || !x) return -1;
+    if (!n_pad) return 0;
+    features<<<(n_pad + 255)/256, 256, 0, (cudaStream_t)stream>>>(
+        n, n_pad, radius, length, rpd, lpd, drho, q, flag, static_cast<__nv_bfloat16 *>(x));
+    return status("features");
+}
+
+}  // extern "C"

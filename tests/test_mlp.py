@@ -1,0 +1,159 @@
+"""
+Surrogate MLP: the numpy oracle checked by finite differences (CPU), then
+the tensor-core forward, backward and weight-gradient kernels checked
+against the oracle, and a short training run (GPU).
+"""
+
+import numpy as np
+import pytest
+
+from oracle import mlp_ref
+
+
+def _random_net(rng, scale=0.5, nin=16, hid=256):
+    W = [rng.normal(0, scale/np.sqrt(nin if l == 0 else hid), (hid, nin if l == 0 else hid))
+         for l in range(4)]
+    W[0][:, 7:] = 0.0
+    b = [rng.normal(0, 0.1, hid) for _ in range(4)]
+    w_out = rng.normal(0, 1/np.sqrt(hid), hid)
+    return W, b, w_out, 0.3
+
+
+def test_oracle_backward_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    hid = 8
+    W = [rng.normal(0, 0.5, (hid, 16 if l == 0 else hid)) for l in range(4)]
+    b = [rng.normal(0, 0.1, hid) for _ in range(4)]
+    w_out = rng.normal(0, 0.5, hid)
+    x = rng.normal(0, 1, (5, 16))
+    dout = rng.normal(0, 1, 5)
+
+    def f(W, b, w_out, b_out):
+        out, _, _ = mlp_ref.forward(x, W, b, w_out, b_out, emulate_bf16=False)
+        return float(dout @ out)
+    out, zs, hs = mlp_ref.forward(x, W, b, w_out, 0.2, emulate_bf16=False)
+    dW, db, dwo, dbo = mlp_ref.backward(x, W, w_out, dout, zs, hs, emulate_bf16=False)
+    eps = 1e-6
+    for l in range(4):
+        for (i, j) in [(0, 0), (3, 5), (hid - 1, 2)]:
+            Wp = [w.copy() for w in W]
+            Wp[l][i, j] += eps
+            Wm = [w.copy() for w in W]
+            Wm[l][i, j] -= eps
+            fd = (f(Wp, b, w_out, 0.2) - f(Wm, b, w_out, 0.2))/(2*eps)
+            assert abs(fd - dW[l][i, j]) < 1e-6*max(1, abs(fd))
+        bp = [v.copy() for v in b]
+        bp[l][1] += eps
+        bm = [v.copy() for v in b]
+        bm[l][1] -= eps
+        fd = (f(W, bp, w_out, 0.2) - f(W, bm, w_out, 0.2))/(2*eps)
+        assert abs(fd - db[l][1]) < 1e-6*max(1, abs(fd))
+    wp = w_out.copy()
+    wp[2] += eps
+    wm = w_out.copy()
+    wm[2] -= eps
+    fd = (f(W, b, wp, 0.2) - f(W, b, wm, 0.2))/(2*eps)
+    assert abs(fd - dwo[2]) < 1e-6
+    assert abs(dbo - dout.sum()) < 1e-12
+
+
+def test_bf16_rounding():
+    x = np.array([1.0, 1.0 + 2**-8, 1.0 + 2**-7, -3.14159, 1e-3])
+    r = mlp_ref.bf16(x)
+    assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2**-7
+    assert abs(r[3] + 3.140625) < 1e-12
+
+
+def _gpu_net(rng):
+    import torch
+    from sasmodels_b200.surrogate import MLP
+    net = MLP(seed=1)
+    W, b, w_out, b_out = _random_net(rng)
+    net.load_state({"W": [w.astype(np.float32) for w in W],
+                    "b": [v.astype(np.float32) for v in b],
+                    "w_out": w_out.astype(np.float32),
+                    "b_out": np.array([b_out], np.float32)})
+    return net, W, b, w_out, b_out
+
+
+def _inputs(rng, n, n_pad):
+    import torch
+    x = np.zeros((n_pad, 16))
+    x[:n, :7] = rng.uniform(-1, 1, (n, 7))
+    xb = mlp_ref.bf16(x)
+    return torch.as_tensor(xb, dtype=torch.bfloat16, device="cuda"), xb
+
+
+@pytest.mark.gpu
+def test_tc_forward_matches_oracle(cuda):
+    rng = np.random.default_rng(3)
+    net, W, b, w_out, b_out = _gpu_net(rng)
+    n, n_pad = 300, 384
+    x, xh = _inputs(rng, n, n_pad)
+    out = net.forward(x, n)
+    net.stream.synchronize()
+    assert net.errors() == 0
+    got = out.cpu().numpy()[:n]
+    ref, _, _ = mlp_ref.forward(xh[:n], [mlp_ref.bf16(w) for w in W],
+                                [np.float32(v).astype(np.float64) for v in b],
+                                np.float32(w_out).astype(np.float64), np.float32(b_out))
+    err = np.abs(got - ref).max()/np.abs(ref).max()
+    assert err < 2e-2, err
+    # an FP64 forward without BF16 storage differs only at BF16 precision
+    exact, _, _ = mlp_ref.forward(xh[:n], W, b, w_out, b_out, emulate_bf16=False)
+    assert np.abs(got - exact).max()/np.abs(exact).max() < 5e-2
+
+
+@pytest.mark.gpu
+def test_tc_gradients_match_oracle(cuda):
+    import torch
+    rng = np.random.default_rng(4)
+    net, W, b, w_out, b_out = _gpu_net(rng)
+    n, n_pad = 500, 512
+    x, xh = _inputs(rng, n, n_pad)
+    y = torch.as_tensor(rng.normal(0, 1, n_pad), dtype=torch.float32, device="cuda")
+    loss, dW, db, dwo, dbo = net.gradients(x, y, n)
+    net.stream.synchronize()
+    assert net.errors() == 0
+    Wf = [np.float32(w).astype(np.float64) for w in W]
+    bf = [np.float32(v).astype(np.float64) for v in b]
+    wof = np.float32(w_out).astype(np.float64)
+    out, zs, hs = mlp_ref.forward(xh, Wf, bf, wof, np.float32(b_out))
+    yv = y.cpu().numpy().astype(np.float64)
+    dout = np.zeros(n_pad)
+    dout[:n] = 2*(out[:n] - yv[:n])/n
+    rW, rb, rwo, rbo = mlp_ref.backward(xh, Wf, wof, dout, zs, hs)
+    for l in range(4):
+        nb = 16 if l == 0 else 256
+        g = dW[l].cpu().numpy().reshape(net.splits, 256, nb).sum(axis=0)
+        rel = np.linalg.norm(g - rW[l])/np.linalg.norm(rW[l])
+        assert rel < 2e-2, (l, rel)
+        rel = np.linalg.norm(db[l].cpu().numpy() - rb[l])/np.linalg.norm(rb[l])
+        assert rel < 2e-2, (l, "bias", rel)
+    rel = np.linalg.norm(dwo.cpu().numpy() - rwo)/np.linalg.norm(rwo)
+    assert rel < 2e-2
+    assert abs(float(dbo.item()) - rbo) < 1e-3*max(1, abs(rbo))
+    assert abs(float(loss.item()) - np.mean((out[:n] - yv[:n])**2)) < 2e-2*np.mean((out[:n] - yv[:n])**2)
+
+
+@pytest.mark.gpu
+def test_tc_training_reduces_loss(cuda):
+    """Fit a smooth function of the 7 inputs; the loss must fall by >10x."""
+    import torch
+    from sasmodels_b200.surrogate import MLP
+    rng = np.random.default_rng(5)
+    net = MLP(seed=2)
+    n = n_pad = 4096
+    xs = np.zeros((n, 16))
+    xs[:, :7] = rng.uniform(-1, 1, (n, 7))
+    target = np.sin(2*xs[:, 0]) + xs[:, 1]*xs[:, 5] - 0.5*xs[:, 3]**2
+    x = torch.as_tensor(xs, dtype=torch.bfloat16, device="cuda")
+    y = torch.as_tensor(target, dtype=torch.float32, device="cuda")
+    first = None
+    for step in range(300):
+        loss = net.train_step(x, y, n, lr=2e-3)
+        if first is None:
+            first = float(loss.item())
+    last = float(loss.item())
+    assert net.errors() == 0
+    assert last < first/10, (first, last)
