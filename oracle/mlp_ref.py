@@ -4,9 +4,9 @@ CPU oracle for the surrogate MLP (test infrastructure only).
 numpy restatement of the forward and backward passes of the tensor-core MLP
 in ``sasmodels_b200/csrc/mlp.cu``: 16 -> 256 -> 256 -> 256 -> 256 -> 1,
 SiLU, z = h W^T + b, out = h3 . w_out + b_out, MSE loss.  With
-``emulate_bf16=True`` every value the GPU stores as BF16 (inputs, weights,
-hidden activations fed to the next layer, saved z/h, dZ) is rounded the same
-way, so the device gradients can be compared tightly; with ``False`` it is
+``emulate_bf16=True`` every value the GPU stores as BF16 (weights, saved
+z/h, dZ; inputs and hidden activations as a compensated hi + lo BF16 pair) is
+rounded the same way, so the device gradients can be compared tightly; with ``False`` it is
 the plain FP64 mathematics the kernels approximate.
 """
 
@@ -30,17 +30,26 @@ def dsilu(z):
     return s*(1.0 + z*(1.0 - s))
 
 
-def forward(x, W, b, w_out, b_out, emulate_bf16=True):
-    """Returns out and the saved (z, h) per hidden layer."""
+def split_bf16(a):
+    """Compensated BF16 pair hi + lo of a, summed (what the kernels feed the
+    tensor cores as two BF16 operands)."""
+    hi = bf16(a)
+    return hi + bf16(np.asarray(a, np.float64) - hi)
+
+
+def forward(x, W, b, w_out, b_out, emulate_bf16=True, split_act=True):
+    """Returns out and the saved (z, h) per hidden layer.  With
+    ``split_act`` the layer inputs carry the compensated hi + lo pair."""
     r = bf16 if emulate_bf16 else (lambda a: np.asarray(a, np.float64))
-    a = r(x)
+    feed = split_bf16 if (emulate_bf16 and split_act) else r
+    a = feed(x)
     zs, hs = [], []
     for l in range(4):
         z = a @ r(W[l]).T + b[l]
         h = silu(z)
         zs.append(r(z))
         hs.append(r(h))
-        a = r(h)
+        a = feed(h)
         last_h = h
     out = last_h @ w_out + b_out
     return out, zs, hs

@@ -5,7 +5,12 @@
 // Kernels
 //   mlp_forward    all four hidden layers of 128 samples per CTA; the
 //                  activations stay in shared memory as the next layer's A
-//                  operand, weights stream through a 256 x 64 staging tile;
+//                  operand, weights stream through a 256 x 64 staging tile.
+//                  Activations are kept as a compensated BF16 pair
+//                  h = hi + lo (hi = bf16(h), lo = bf16(h - hi)) and each
+//                  layer issues the MMAs of both halves into the same FP32
+//                  accumulator, so the layer inputs carry ~16 significant
+//                  bits instead of 8 while every operand stays BF16;
 //                  bias + SiLU in the TMEM epilogue, the 256 -> 1 output layer
 //                  as a per-row dot product in the last epilogue.  Optionally
 //                  saves the pre-activations z and activations h for training.
@@ -14,7 +19,7 @@
 //                  way (A = dZ in smem, B = W_l^T streamed).
 //   gemm_nt        C_split = A[M x K] B[N x K]^T over a K range (split-K):
 //                  weight gradients dW = dZ^T H with the batch as K.
-//   + transpose, row sums/dots, MSE gradient, Adam, feature packing.
+//   + transpose, row sums/dots, loss gradient, Adam, feature packing.
 //
 // All launches return an error code; device-side waits are bounded and
 // report through *err (0 = ok).
@@ -32,7 +37,9 @@ constexpr int NIN = 16;           // padded input features
 constexpr int TM = 128;           // rows per CTA
 constexpr int KC = 64;            // streamed K chunk
 constexpr int THREADS = 128;
-constexpr int FWD_SMEM = TM*HID*2 + HID*KC*2;      // 64 KB act + 32 KB weights
+constexpr int ACT_BYTES = TM*HID*2;                // one 128 x 256 bf16 tile
+constexpr int FWD_SMEM = 2*ACT_BYTES + HID*KC*2;   // act hi + lo + 32 KB weights
+constexpr int BWD_SMEM = ACT_BYTES + HID*KC*2;     // dZ tile + 32 KB weights
 constexpr int GEMM_SMEM = 100*1024;                // keeps <= 2 CTAs per SM (TMEM)
 
 struct Weights {
@@ -83,9 +90,11 @@ struct Pipe {
 // Issue the MMAs of one staged chunk (single thread), then wait (all).
 // a_addr: canonical 128-row A tile holding the full K; a_step0: first K=16
 // step of this chunk within A; b_addr: canonical NB-row tile of this chunk.
+// a_lo_addr != 0 adds the MMAs of the low half of a compensated A.
 template <int NB, int STEPS>
 __device__ __forceinline__ void mma_chunk(Pipe &pp, uint32_t tmem, uint32_t a_addr, int a_step0,
-                                          uint32_t b_addr, bool accumulate)
+                                          uint32_t b_addr, bool accumulate,
+                                          uint32_t a_lo_addr = 0)
 {
     tc::fence_async_smem();
     tc::fence_before_sync();
@@ -95,9 +104,11 @@ __device__ __forceinline__ void mma_chunk(Pipe &pp, uint32_t tmem, uint32_t a_ad
         constexpr uint32_t idesc = tc::idesc_bf16(128, NB);
         #pragma unroll
         for (int s = 0; s < STEPS; ++s) {
-            tc::mma_bf16(tmem, tc::kmajor_desc<128>(a_addr, a_step0 + s),
-                         tc::kmajor_desc<NB>(b_addr, s), idesc,
+            const uint64_t bdesc = tc::kmajor_desc<NB>(b_addr, s);
+            tc::mma_bf16(tmem, tc::kmajor_desc<128>(a_addr, a_step0 + s), bdesc, idesc,
                          (accumulate || s > 0) ? 1u : 0u);
+            if (a_lo_addr)
+                tc::mma_bf16(tmem, tc::kmajor_desc<128>(a_lo_addr, a_step0 + s), bdesc, idesc, 1u);
         }
         tc::mma_commit(pp.bar);
     }
@@ -107,15 +118,17 @@ __device__ __forceinline__ void mma_chunk(Pipe &pp, uint32_t tmem, uint32_t a_ad
     tc::fence_after_sync();
 }
 
-// A (128 x 256, resident) times a streamed [256 x 256] weight (rows = N).
+// A (128 x 256, resident; plus its low half when act_lo != nullptr) times a
+// streamed [256 x 256] weight (rows = N).
 __device__ __forceinline__ void layer_256(Pipe &pp, uint32_t tmem, uint8_t *act, uint8_t *wbuf,
-                                          const __nv_bfloat16 *w)
+                                          const __nv_bfloat16 *w, uint8_t *act_lo = nullptr)
 {
     const uint32_t a_addr = tc::smem_u32(act), b_addr = tc::smem_u32(wbuf);
+    const uint32_t lo_addr = act_lo ? tc::smem_u32(act_lo) : 0u;
     for (int kc = 0; kc < HID/KC; ++kc) {
         if (!pp.ok) return;
         load_tile<HID, KC>(wbuf, w, HID, kc*KC, HID);
-        mma_chunk<HID, KC/16>(pp, tmem, a_addr, kc*(KC/16), b_addr, kc > 0);
+        mma_chunk<HID, KC/16>(pp, tmem, a_addr, kc*(KC/16), b_addr, kc > 0, lo_addr);
     }
 }
 
@@ -141,6 +154,20 @@ __device__ __forceinline__ void store16(uint8_t *act, int row, int c0, const flo
     *reinterpret_cast<uint4 *>(act + tc::kmajor_offset<TM>(row, c0 + 8)) = hi;
 }
 
+// Compensated pair: hi = bf16(h) into act, lo = bf16(h - hi) into act_lo.
+__device__ __forceinline__ void store16_split(uint8_t *act, uint8_t *act_lo, int row, int c0,
+                                              const float (&h)[16])
+{
+    float hi[16], lo[16];
+    #pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        hi[j] = __bfloat162float(__float2bfloat16_rn(h[j]));
+        lo[j] = h[j] - hi[j];
+    }
+    store16(act, row, c0, hi);
+    store16(act_lo, row, c0, lo);
+}
+
 __device__ __forceinline__ void save16(__nv_bfloat16 *dst, const float (&h)[16])
 {
     uint4 lo, hi;
@@ -164,7 +191,8 @@ __device__ __forceinline__ void load16(const __nv_bfloat16 *src, float (&z)[16])
 // Epilogue of hidden layer l: z = acc + b, h = silu(z); h back into the
 // activation tile (next A), z and h optionally to global; the last layer
 // also forms out = h . w_out + b_out.
-__device__ __forceinline__ void epilogue_hidden(uint32_t tmem, uint8_t *act, const float *bias,
+__device__ __forceinline__ void epilogue_hidden(uint32_t tmem, uint8_t *act, uint8_t *act_lo,
+                                                const float *bias,
                                                 const float *w_out, const float *b_out, bool last,
                                                 int grow, int n, __nv_bfloat16 *zs,
                                                 __nv_bfloat16 *hs, float *out)
@@ -183,7 +211,7 @@ __device__ __forceinline__ void epilogue_hidden(uint32_t tmem, uint8_t *act, con
             #pragma unroll
             for (int j = 0; j < 16; ++j) dot = fmaf(h[j], w_out[c0 + j], dot);
         } else {
-            store16(act, t, c0, h);
+            store16_split(act, act_lo, t, c0, h);
         }
         if (zs != nullptr) {          // every row of the padded batch (zero inputs)
             save16(zs + (size_t)grow*HID + c0, z);
@@ -194,13 +222,15 @@ __device__ __forceinline__ void epilogue_hidden(uint32_t tmem, uint8_t *act, con
 }
 
 __global__ void __launch_bounds__(THREADS, 1)
-mlp_forward(int n, const __nv_bfloat16 *__restrict__ x, Weights wts, float *__restrict__ out,
+mlp_forward(int n, const __nv_bfloat16 *__restrict__ x, const __nv_bfloat16 *__restrict__ x_lo,
+            Weights wts, float *__restrict__ out,
             __nv_bfloat16 *__restrict__ z_save, __nv_bfloat16 *__restrict__ h_save,
             int *__restrict__ err)
 {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t *act = smem;
-    uint8_t *wbuf = smem + TM*HID*2;
+    uint8_t *act_lo = smem + ACT_BYTES;
+    uint8_t *wbuf = smem + 2*ACT_BYTES;
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmem_slot;
     const int t = threadIdx.x;
@@ -220,15 +250,17 @@ mlp_forward(int n, const __nv_bfloat16 *__restrict__ x, Weights wts, float *__re
     const uint32_t tmem = tmem_slot;
     Pipe pp{&bar, 0u, true};
 
-    // layer 0: K = 16 (7 features + zero padding)
+    // layer 0: K = 16 features (hi and lo halves)
     load_tile<TM, NIN>(act, x + (size_t)row0*NIN, NIN, 0, n - row0);
+    load_tile<TM, NIN>(act_lo, x_lo + (size_t)row0*NIN, NIN, 0, n - row0);
     load_tile<HID, NIN>(wbuf, wts.w[0], NIN, 0, HID);
-    mma_chunk<HID, 1>(pp, tmem, tc::smem_u32(act), 0, tc::smem_u32(wbuf), false);
+    mma_chunk<HID, 1>(pp, tmem, tc::smem_u32(act), 0, tc::smem_u32(wbuf), false,
+                      tc::smem_u32(act_lo));
     const size_t plane = (size_t)gridDim.x*TM*HID;
     for (int l = 0; l < 4 && pp.ok; ++l) {
-        if (l > 0) layer_256(pp, tmem, act, wbuf, wts.w[l]);
+        if (l > 0) layer_256(pp, tmem, act, wbuf, wts.w[l], act_lo);
         if (!pp.ok) break;
-        epilogue_hidden(tmem, act, wts.b[l], wts.w_out, wts.b_out, l == 3, row0 + t, n,
+        epilogue_hidden(tmem, act, act_lo, wts.b[l], wts.w_out, wts.b_out, l == 3, row0 + t, n,
                         z_save ? z_save + l*plane : nullptr,
                         h_save ? h_save + l*plane : nullptr, out);
         tc::fence_before_sync();
@@ -255,7 +287,7 @@ mlp_backward(int n, WeightsT wts, const float *__restrict__ dout,
 {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t *act = smem;
-    uint8_t *wbuf = smem + TM*HID*2;
+    uint8_t *wbuf = smem + ACT_BYTES;
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmem_slot;
     const int t = threadIdx.x;
@@ -411,16 +443,27 @@ __global__ void row_dot(int rows, int cols, const __nv_bfloat16 *__restrict__ M,
     if (lane == 0) out[r] = s;
 }
 
-// dout = 2 (out - y) / n on the first n rows, 0 on padding; loss partials
-__global__ void mse_grad(int n, int n_pad, const float *__restrict__ out,
-                         const float *__restrict__ y, float *__restrict__ dout,
-                         float *__restrict__ sq)
+// Gradient of the mean loss over the first n rows (0 on padding) and the
+// per-row loss: squared error for delta <= 0, else Huber with threshold
+// delta (quadratic inside, linear outside), which keeps the few points
+// near form-factor minima from dominating the fit.
+__global__ void loss_grad(int n, int n_pad, const float *__restrict__ out,
+                          const float *__restrict__ y, float delta, float *__restrict__ dout,
+                          float *__restrict__ loss)
 {
     const int i = blockIdx.x*blockDim.x + threadIdx.x;
     if (i >= n_pad) return;
     const float d = i < n ? out[i] - y[i] : 0.0f;
-    dout[i] = i < n ? 2.0f*d/(float)n : 0.0f;
-    sq[i] = d*d;
+    float g, l;
+    if (delta <= 0.0f || fabsf(d) <= delta) {
+        g = 2.0f*d;
+        l = d*d;
+    } else {
+        g = 2.0f*delta*copysignf(1.0f, d);
+        l = delta*(2.0f*fabsf(d) - delta);
+    }
+    dout[i] = i < n ? g/(float)n : 0.0f;
+    loss[i] = l;
 }
 
 // Adam on one FP32 master tensor; grad = sum of `splits` partial gradients.
@@ -447,14 +490,19 @@ __global__ void adam_step(int size, int splits, const float *__restrict__ grad, 
     }
 }
 
-// Surrogate input features (7 used of 16), each mapped to [-1, 1]:
-//   log R on [log 10, log 300], log L on [log 20, log 3000], R_pd and L_pd on
-//   [0, 0.3], contrast on [-5, 5], log q on [log 1e-3, log 0.5], flag {0, 1}.
+// Surrogate input features, each mapped to about [-1, 1]: the seven model
+// inputs -- log R on [log 10, log 300], log L on [log 20, log 3000], R_pd and
+// L_pd on [0, 0.3], contrast on [-5, 5], log q on [log 1e-3, log 0.5], flag
+// {0, 1} -- and four functions of them that carry the scattering physics in
+// a form a small network represents easily: log(qR), log(qL/2) and the
+// dispersity damping log(1 + R_pd qR), log(1 + L_pd qL/2), and the damped
+// oscillations cos/sin(2qR) exp(-2 (R_pd qR)^2), cos/sin(qL) exp(-2 (L_pd qL/2)^2).
+// Slot 15 is zero.
 __global__ void features(int n, int n_pad, const double *__restrict__ radius,
                          const double *__restrict__ length, const double *__restrict__ rpd,
                          const double *__restrict__ lpd, const double *__restrict__ drho,
                          const double *__restrict__ q, const double *__restrict__ flag,
-                         __nv_bfloat16 *__restrict__ x)
+                         __nv_bfloat16 *__restrict__ x, __nv_bfloat16 *__restrict__ x_lo)
 {
     const int i = blockIdx.x*blockDim.x + threadIdx.x;
     if (i >= n_pad) return;
@@ -469,10 +517,25 @@ __global__ void features(int n, int n_pad, const double *__restrict__ radius,
         f[4] = (float)(drho[i]/5.0);
         f[5] = (float)(2.0*(log(q[i]) - log(1e-3))/(log(0.5) - log(1e-3)) - 1.0);
         f[6] = (float)(2.0*flag[i] - 1.0);
+        const double qr = q[i]*radius[i], qh = 0.5*q[i]*length[i];
+        f[7] = (float)(log(qr)/4.0);
+        f[8] = (float)(log(qh)/4.0);
+        f[9] = (float)(log1p(rpd[i]*qr)/2.0);
+        f[10] = (float)(log1p(lpd[i]*qh)/2.0);
+        // oscillation of the cross-section and length factors (period pi in
+        // qR and qL/2), damped as a gaussian size distribution damps them
+        const double ar = exp(-2.0*(rpd[i]*qr)*(rpd[i]*qr));
+        const double al = exp(-2.0*(lpd[i]*qh)*(lpd[i]*qh));
+        f[11] = (float)(ar*cos(2.0*qr));
+        f[12] = (float)(ar*sin(2.0*qr));
+        f[13] = (float)(al*cos(2.0*qh));
+        f[14] = (float)(al*sin(2.0*qh));
     }
-    uint4 *dst = reinterpret_cast<uint4 *>(x + (size_t)i*NIN);
-    dst[0] = make_uint4(pack2(f[0], f[1]), pack2(f[2], f[3]), pack2(f[4], f[5]), pack2(f[6], f[7]));
-    dst[1] = make_uint4(pack2(f[8], f[9]), pack2(f[10], f[11]), pack2(f[12], f[13]), pack2(f[14], f[15]));
+    float lo[16];
+    #pragma unroll
+    for (int j = 0; j < 16; ++j) lo[j] = f[j] - __bfloat162float(__float2bfloat16_rn(f[j]));
+    save16(x + (size_t)i*NIN, f);
+    save16(x_lo + (size_t)i*NIN, lo);
 }
 
 inline char *errbuf()
@@ -501,12 +564,14 @@ const char *sasb200_mlp_last_error(void) { return errbuf(); }
 
 // out[n] (and z/h planes [4][n_pad x 256] when non-null) for x[n_pad x 16];
 // n_pad a multiple of 128.
-int32_t sasb200_mlp_forward(int32_t n, int32_t n_pad, const void *x, const void *const *w,
+int32_t sasb200_mlp_forward(int32_t n, int32_t n_pad, const void *x, const void *x_lo,
+                            const void *const *w,
                             const float *const *b, const float *w_out, const float *b_out, float *out,
                             void *z_save, void *h_save, int32_t *err, void *stream)
 {
     errbuf()[0] = 0;
-    if (n < 0 || n_pad % TM || n > n_pad || !x || !w || !b || !w_out || !b_out || !out || !err)
+    if (n < 0 || n_pad % TM || n > n_pad || !x || !x_lo || !w || !b || !w_out || !b_out || !out
+        || !err)
         return (std::snprintf(errbuf(), 256, "bad arguments"), -1);
     if ((z_save == nullptr) != (h_save == nullptr))
         return (std::snprintf(errbuf(), 256, "z_save and h_save go together"), -1);
@@ -520,7 +585,7 @@ int32_t sasb200_mlp_forward(int32_t n, int32_t n_pad, const void *x, const void 
     wts.b_out = b_out;
     cudaFuncSetAttribute(mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM);
     mlp_forward<<<n_pad/TM, THREADS, FWD_SMEM, (cudaStream_t)stream>>>(
-        n, static_cast<const __nv_bfloat16 *>(x), wts, out,
+        n, static_cast<const __nv_bfloat16 *>(x), static_cast<const __nv_bfloat16 *>(x_lo), wts, out,
         static_cast<__nv_bfloat16 *>(z_save), static_cast<__nv_bfloat16 *>(h_save), err);
     return status("mlp_forward");
 }
@@ -536,8 +601,8 @@ int32_t sasb200_mlp_backward(int32_t n, int32_t n_pad, const void *const *wt, co
     WeightsT wts;
     for (int l = 0; l < 4; ++l) wts.wt[l] = static_cast<const __nv_bfloat16 *>(wt[l]);
     wts.w_out = w_out;
-    cudaFuncSetAttribute(mlp_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM);
-    mlp_backward<<<n_pad/TM, THREADS, FWD_SMEM, (cudaStream_t)stream>>>(
+    cudaFuncSetAttribute(mlp_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, BWD_SMEM);
+    mlp_backward<<<n_pad/TM, THREADS, BWD_SMEM, (cudaStream_t)stream>>>(
         n, wts, dout, static_cast<const __nv_bfloat16 *>(z_save),
         static_cast<__nv_bfloat16 *>(dz_save), err);
     return status("mlp_backward");
@@ -591,13 +656,14 @@ int32_t sasb200_row_dot(int32_t rows, int32_t cols, const void *M, const float *
     return status("row_dot");
 }
 
-int32_t sasb200_mse_grad(int32_t n, int32_t n_pad, const float *out, const float *y, float *dout,
-                         float *sq, void *stream)
+int32_t sasb200_loss_grad(int32_t n, int32_t n_pad, const float *out, const float *y, float delta,
+                          float *dout, float *loss, void *stream)
 {
-    if (n < 0 || n > n_pad || !out || !y || !dout || !sq) return -1;
+    if (n < 0 || n > n_pad || !out || !y || !dout || !loss) return -1;
     if (!n_pad) return 0;
-    mse_grad<<<(n_pad + 255)/256, 256, 0, (cudaStream_t)stream>>>(n, n_pad, out, y, dout, sq);
-    return status("mse_grad");
+    loss_grad<<<(n_pad + 255)/256, 256, 0, (cudaStream_t)stream>>>(n, n_pad, out, y, delta,
+                                                                   dout, loss);
+    return status("loss_grad");
 }
 
 int32_t sasb200_adam(int32_t size, int32_t splits, const float *grad, float *p, float *m, float *v,
@@ -615,12 +681,14 @@ int32_t sasb200_adam(int32_t size, int32_t splits, const float *grad, float *p, 
 
 int32_t sasb200_mlp_features(int32_t n, int32_t n_pad, const double *radius, const double *length,
                              const double *rpd, const double *lpd, const double *drho,
-                             const double *q, const double *flag, void *x, void *stream)
+                             const double *q, const double *flag, void *x, void *x_lo,
+                             void *stream)
 {
-    if (n < 0 || n > n_pad || !x) return -1;
+    if (n < 0 || n > n_pad || !x || !x_lo) return -1;
     if (!n_pad) return 0;
     features<<<(n_pad + 255)/256, 256, 0, (cudaStream_t)stream>>>(
-        n, n_pad, radius, length, rpd, lpd, drho, q, flag, static_cast<__nv_bfloat16 *>(x));
+        n, n_pad, radius, length, rpd, lpd, drho, q, flag, static_cast<__nv_bfloat16 *>(x),
+        static_cast<__nv_bfloat16 *>(x_lo));
     return status("features");
 }
 

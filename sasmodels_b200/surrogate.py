@@ -13,8 +13,8 @@ its judge and its fallback.
   at theta = 90, phi = 0 without jitter, with q along qx.
 * The intensity is exactly quadratic in the contrast, so the network learns
   y = log I at unit contrast and ``2 log|contrast|`` is added back.
-* Predicted error: a calibration table of the held-out |error| (99th
-  percentile) over (log q, log L, log R) bins.  Points whose predicted error
+* Predicted error: a calibration table of the held-out |error| (95th
+  percentile) over (log qR, log qL/2, R_pd, L_pd, flag) bins.  Points whose predicted error
   exceeds the tolerance (default 1 % in log I), or that fall outside the
   training domain, are recomputed by the plain kernel.
 
@@ -45,16 +45,16 @@ def _lib():
         raise RuntimeError("surrogate library not built: %s" % path)
     lib = ct.CDLL(path)
     P, I, F = ct.c_void_p, ct.c_int32, ct.c_float
-    lib.sasb200_mlp_forward.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P]
+    lib.sasb200_mlp_forward.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P, P]
     lib.sasb200_mlp_backward.argtypes = [I, I, P, P, P, P, P, P, P]
     lib.sasb200_gemm_nt.argtypes = [I, I, I, I, I, P, P, I, P, P, P]
     lib.sasb200_transpose_bf16.argtypes = [I, I, P, P, P]
     lib.sasb200_row_dot.argtypes = [I, I, P, P, P, P]
-    lib.sasb200_mse_grad.argtypes = [I, I, P, P, P, P, P]
+    lib.sasb200_loss_grad.argtypes = [I, I, P, P, F, P, P, P]
     lib.sasb200_adam.argtypes = [I, I, P, P, P, P, F, F, F, F, I, P, P, I, I, P]
-    lib.sasb200_mlp_features.argtypes = [I, I, P, P, P, P, P, P, P, P, P]
+    lib.sasb200_mlp_features.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P]
     for name in ("sasb200_mlp_forward", "sasb200_mlp_backward", "sasb200_gemm_nt",
-                 "sasb200_transpose_bf16", "sasb200_row_dot", "sasb200_mse_grad",
+                 "sasb200_transpose_bf16", "sasb200_row_dot", "sasb200_loss_grad",
                  "sasb200_adam", "sasb200_mlp_features"):
         getattr(lib, name).restype = I
     lib.sasb200_mlp_last_error.restype = ct.c_char_p
@@ -81,11 +81,11 @@ class MLP:
         f32 = dict(dtype=torch.float32, device=self.device)
         self.W, self.b = [], []
         for l, (o, i) in enumerate(shapes):
-            fan_in = 7 if l == 0 else i
+            fan_in = 15 if l == 0 else i
             bound = math.sqrt(6.0/fan_in)
             w = rng.uniform(-bound, bound, (o, i))
             if l == 0:
-                w[:, 7:] = 0.0
+                w[:, 15:] = 0.0
             self.W.append(torch.as_tensor(w, **f32))
             self.b.append(torch.zeros(o, **f32))
         self.w_out = torch.as_tensor(rng.uniform(-1, 1, HID)/math.sqrt(HID), **f32)
@@ -94,6 +94,8 @@ class MLP:
         self.m = [torch.zeros_like(p) for p in self.params]
         self.v = [torch.zeros_like(p) for p in self.params]
         self.step_count = 0
+        #: Huber threshold of the training loss (<= 0: squared error)
+        self.huber = 0.0
         self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
         self._sync_bf16()
         self._scratch_n = 0
@@ -136,20 +138,22 @@ class MLP:
         self._scratch_n = n_pad
 
     # ----------------------------------------------------------- kernels --
-    def forward(self, x, n, save=False):
-        """out[n_pad] for features x (bf16 [n_pad x 16]), on self.stream."""
+    def forward(self, x, x_lo, n, save=False):
+        """out[n_pad] for features x + x_lo (bf16 [n_pad x 16] each), on
+        self.stream."""
         n_pad = x.shape[0]
         self._scratch(n_pad)
         st = self.stream.cuda_stream
         w = self._ptrs(self.Wb)
         b = self._ptrs(self.b)
         self._check(self.lib.sasb200_mlp_forward(
-            n, n_pad, x.data_ptr(), w, b, self.w_out.data_ptr(), self.b_out.data_ptr(),
+            n, n_pad, x.data_ptr(), x_lo.data_ptr(), w, b, self.w_out.data_ptr(),
+            self.b_out.data_ptr(),
             self.out.data_ptr(), self.z_save.data_ptr() if save else None,
             self.h_save.data_ptr() if save else None, self.err.data_ptr(), st), "mlp_forward")
         return self.out[:n_pad]
 
-    def gradients(self, x, y, n):
+    def gradients(self, x, x_lo, y, n):
         """Loss and gradients of one batch, all on self.stream: returns
         (loss, dW split partials [4], db [4], dw_out, db_out)."""
         torch = self.torch
@@ -158,11 +162,12 @@ class MLP:
         st = self.stream.cuda_stream
         lib = self.lib
         self._check(lib.sasb200_mlp_forward(
-            n, n_pad, x.data_ptr(), self._ptrs(self.Wb), self._ptrs(self.b),
+            n, n_pad, x.data_ptr(), x_lo.data_ptr(), self._ptrs(self.Wb), self._ptrs(self.b),
             self.w_out.data_ptr(), self.b_out.data_ptr(), self.out.data_ptr(),
             self.z_save.data_ptr(), self.h_save.data_ptr(), self.err.data_ptr(), st), "forward")
-        self._check(lib.sasb200_mse_grad(n, n_pad, self.out.data_ptr(), y.data_ptr(),
-                                         self.dout.data_ptr(), self.sq.data_ptr(), st), "mse")
+        self._check(lib.sasb200_loss_grad(n, n_pad, self.out.data_ptr(), y.data_ptr(),
+                                          float(self.huber), self.dout.data_ptr(),
+                                          self.sq.data_ptr(), st), "loss")
         self._check(lib.sasb200_mlp_backward(n, n_pad, self._ptrs(self.WTb), self.w_out.data_ptr(),
                                              self.dout.data_ptr(), self.z_save.data_ptr(),
                                              self.dz_save.data_ptr(), self.err.data_ptr(), st),
@@ -195,8 +200,8 @@ class MLP:
             loss = self.sq[:n].mean()
         return loss, self.gW, self.gb, self.gw, self.gbo
 
-    def train_step(self, x, y, n, lr, b1=0.9, b2=0.999, eps=1e-8):
-        loss, dW, db, gw, gbo = self.gradients(x, y, n)
+    def train_step(self, x, x_lo, y, n, lr, b1=0.9, b2=0.999, eps=1e-8):
+        loss, dW, db, gw, gbo = self.gradients(x, x_lo, y, n)
         self.step_count += 1
         st = self.stream.cuda_stream
         lib = self.lib
@@ -215,18 +220,21 @@ class MLP:
         return loss
 
     def features(self, radius, length, rpd, lpd, contrast, q, flag):
-        """bf16 [n_pad x 16] features on the device from float64 arrays."""
+        """Compensated bf16 features (hi, lo) [n_pad x 16] on the device from
+        float64 arrays."""
         torch = self.torch
         n = len(q)
         n_pad = pad128(n)
         arrs = [torch.as_tensor(np.ascontiguousarray(a, 'd'), device=self.device)
                 for a in (radius, length, rpd, lpd, contrast, q, flag)]
         x = torch.empty((n_pad, NIN), dtype=torch.bfloat16, device=self.device)
+        x_lo = torch.empty((n_pad, NIN), dtype=torch.bfloat16, device=self.device)
         with torch.cuda.stream(self.stream):
             self._check(self.lib.sasb200_mlp_features(n, n_pad, *[a.data_ptr() for a in arrs],
-                                                      x.data_ptr(), self.stream.cuda_stream),
+                                                      x.data_ptr(), x_lo.data_ptr(),
+                                                      self.stream.cuda_stream),
                         "features")
-        return x, n
+        return x, x_lo, n
 
     def errors(self):
         return int(self.err.item())
@@ -245,3 +253,325 @@ class MLP:
         self.w_out.copy_(torch.as_tensor(st["w_out"]))
         self.b_out.copy_(torch.as_tensor(st["b_out"]).reshape(1))
         self._sync_bf16()
+
+
+# --------------------------------------------------------------------------
+# data, training, calibration and inference with fallback
+# --------------------------------------------------------------------------
+
+def sample_sets(n_sets, rng, flag=None):
+    """Parameter sets drawn over the training domain (log-uniform sizes,
+    uniform polydispersities and contrast, random orientation flag)."""
+    lo, hi = DOMAIN["radius"]
+    R = np.exp(rng.uniform(np.log(lo), np.log(hi), n_sets))
+    lo, hi = DOMAIN["length"]
+    L = np.exp(rng.uniform(np.log(lo), np.log(hi), n_sets))
+    rpd = rng.uniform(*DOMAIN["rpd"], n_sets)
+    lpd = rng.uniform(*DOMAIN["lpd"], n_sets)
+    contrast = rng.uniform(*DOMAIN["contrast"], n_sets)
+    f = rng.integers(0, 2, n_sets) if flag is None else np.full(n_sets, flag)
+    return dict(radius=R, length=L, rpd=rpd, lpd=lpd, contrast=contrast, flag=f)
+
+
+def sample_q(nq, rng):
+    lo, hi = DOMAIN["q"]
+    return np.sort(np.exp(rng.uniform(np.log(lo), np.log(hi), nq)))
+
+
+def model_pars(R, L, rpd, lpd, flag):
+    """Parameters of the plain cylinder at unit contrast (scale 1, no
+    background); dispersity 35 points over 3 sigma when the width is > 0."""
+    p = dict(radius=float(R), length=float(L), sld=1.0, sld_solvent=0.0,
+             scale=1.0, background=0.0)
+    if rpd > 0:
+        p.update(radius_pd=float(rpd), radius_pd_n=PD_N, radius_pd_nsigma=3.0)
+    if lpd > 0:
+        p.update(length_pd=float(lpd), length_pd_n=PD_N, length_pd_nsigma=3.0)
+    if not flag:
+        p.update(theta=90.0, phi=0.0)
+    return p
+
+
+def plain_unit_iq(sets, qs, device=None, form="float32c"):
+    """I(q) at unit contrast from the plain engines, one array per set:
+    flag 1 through the batched 1D engine, flag 0 through the 2D kernel at
+    theta = 90, phi = 0 with q along qx."""
+    from .batch import Population
+    from .core import load_model
+    n = len(qs)
+    out = [None]*n
+    idx1 = [k for k in range(n) if sets["flag"][k]]
+    if idx1:
+        members = [(qs[k], model_pars(sets["radius"][k], sets["length"][k], sets["rpd"][k],
+                                      sets["lpd"][k], 1)) for k in idx1]
+        pop = Population("cylinder", members, form=form, device=device)
+        pop.run()
+        for k, iq in zip(idx1, pop.iq()):
+            out[k] = iq.copy()
+    idx0 = [k for k in range(n) if not sets["flag"][k]]
+    if idx0:
+        from .direct_model import call_kernel
+        model = load_model("cylinder", dtype="double" if form == "double" else "float32c",
+                           device=device)
+        for k in idx0:
+            q = qs[k]
+            kernel = model.make_kernel([q, np.zeros_like(q)], reorder=False)
+            pars = model_pars(sets["radius"][k], sets["length"][k], sets["rpd"][k],
+                              sets["lpd"][k], 0)
+            out[k] = call_kernel(kernel, pars)
+            kernel.release()
+    return out
+
+
+def flatten(sets, qs):
+    """Flat per-point arrays of (set parameters, q); "set" is the index of
+    the parameter set each point belongs to."""
+    counts = np.array([len(q) for q in qs])
+    cols = {key: np.repeat(np.asarray(sets[key]), counts)
+            for key in ("radius", "length", "rpd", "lpd", "contrast", "flag")}
+    cols["q"] = np.concatenate(qs)
+    cols["set"] = np.repeat(np.arange(len(qs)), counts)
+    return cols
+
+
+class Surrogate:
+    """Trained network + target scaling + error calibration table."""
+
+    TOL = 0.01
+
+    def __init__(self, device=None, seed=0):
+        self.net = MLP(device=device, seed=seed)
+        self.torch = self.net.torch
+        self.y_mean = 0.0
+        self.y_std = 1.0
+        self.table = None
+        self.edges = None
+
+    # ---- data --------------------------------------------------------------
+    def dataset(self, n_sets, nq, seed, form="float32c"):
+        rng = np.random.default_rng(seed)
+        sets = sample_sets(n_sets, rng)
+        qs = [sample_q(nq, rng) for _ in range(n_sets)]
+        iq = plain_unit_iq(sets, qs, self.net.device, form)
+        cols = flatten(sets, qs)
+        y = np.log(np.concatenate(iq))
+        return cols, y
+
+    def _x(self, cols):
+        return self.net.features(cols["radius"], cols["length"], cols["rpd"], cols["lpd"],
+                                 cols["contrast"], cols["q"], cols["flag"].astype(float))
+
+    # ---- training ----------------------------------------------------------
+    def fit(self, cols, y, epochs=8, batch=8192, lr=2e-3, seed=0, log=None, huber=0.05):
+        torch = self.torch
+        good = np.isfinite(y)
+        cols = {k: v[good] for k, v in cols.items()}
+        y = y[good]
+        self.y_mean = float(y.mean())
+        self.y_std = float(y.std())
+        self.net.huber = huber/self.y_std
+        x_all, xlo_all, n = self._x(cols)
+        y_all = torch.as_tensor((y - self.y_mean)/self.y_std, dtype=torch.float32,
+                                device=self.net.device)
+        rng = np.random.default_rng(seed)
+        steps = max(1, n//batch)
+        total = epochs*steps
+        step = 0
+        losses = []
+        for ep in range(epochs):
+            perm = torch.as_tensor(rng.permutation(n), device=self.net.device)
+            for s in range(steps):
+                idx = perm[s*batch:(s + 1)*batch]
+                with torch.cuda.stream(self.net.stream):
+                    xb = x_all.index_select(0, idx)
+                    xlb = xlo_all.index_select(0, idx)
+                    yb = y_all.index_select(0, idx)
+                # cosine decay with a short warm-up
+                frac = step/total
+                rate = lr*min(1.0, (step + 1)/200)*0.5*(1 + math.cos(math.pi*frac))
+                loss = self.net.train_step(xb, xlb, yb, batch, rate)
+                step += 1
+            self.net.stream.synchronize()
+            losses.append(float(loss.item())*self.y_std**2)
+            if log:
+                log("epoch %d loss %.3e" % (ep, losses[-1]))
+        if self.net.errors():
+            raise RuntimeError("tensor-core kernel reported a timeout")
+        return losses
+
+    # ---- inference ----------------------------------------------------------
+    def predict_log(self, cols):
+        """Predicted log I (with the contrast) for flat arrays of inputs."""
+        torch = self.torch
+        x, x_lo, n = self._x(cols)
+        with torch.cuda.stream(self.net.stream):
+            out = self.net.forward(x, x_lo, n)[:n].double()
+            out = out*self.y_std + self.y_mean
+        self.net.stream.synchronize()
+        logc = 2.0*np.log(np.abs(cols["contrast"]))
+        return out.cpu().numpy() + logc
+
+    def _bins(self, cols):
+        """Calibration bin of each point: log(qR), log(qL/2), R_pd, L_pd,
+        flag -- the quantities the network's error follows."""
+        vals = (np.log(cols["q"]*cols["radius"]), np.log(0.5*cols["q"]*cols["length"]),
+                cols["rpd"], cols["lpd"])
+        k = [np.clip(np.searchsorted(e, v) - 1, 0, len(e) - 2)
+             for e, v in zip(self.edges, vals)]
+        return tuple(k) + (cols["flag"].astype(int),)
+
+    def calibrate(self, cols, y_true, quantile=0.95, nbins=(14, 14, 4, 4), min_count=25):
+        """Error table: the `quantile` of |log I error| per bin of a
+        held-out set judged by the plain kernel; bins with fewer than
+        `min_count` points predict infinity (always fall back)."""
+        pred = self.predict_log(cols) - 2.0*np.log(np.abs(cols["contrast"]))
+        err = np.abs(pred - y_true)
+        q0, q1 = DOMAIN["q"]
+        lims = [(np.log(q0*DOMAIN["radius"][0]), np.log(q1*DOMAIN["radius"][1])),
+                (np.log(0.5*q0*DOMAIN["length"][0]), np.log(0.5*q1*DOMAIN["length"][1])),
+                DOMAIN["rpd"], DOMAIN["lpd"]]
+        self.edges = [np.linspace(lo, hi, nb + 1) for (lo, hi), nb in zip(lims, nbins)]
+        keys = self._bins(cols)
+        shape = tuple(nbins) + (2,)
+        flat = np.ravel_multi_index(keys, shape)
+        table = np.full(int(np.prod(shape)), np.inf)
+        order = np.argsort(flat, kind="stable")
+        sf, se = flat[order], err[order]
+        starts = np.flatnonzero(np.r_[True, sf[1:] != sf[:-1]])
+        ends = np.r_[starts[1:], len(sf)]
+        for a, b in zip(starts, ends):
+            if b - a >= min_count:
+                table[sf[a]] = np.quantile(se[a:b], quantile)
+        self.table = table.reshape(shape)
+        return err
+
+    def predicted_error(self, cols):
+        inside = np.ones(len(cols["q"]), bool)
+        for key in ("radius", "length", "rpd", "lpd", "contrast", "q"):
+            lo, hi = DOMAIN[key]
+            inside &= (cols[key] >= lo) & (cols[key] <= hi)
+        inside &= np.abs(cols["contrast"]) > 0
+        pe = self.table[self._bins(cols)]
+        return np.where(inside, pe, np.inf)
+
+    def iq(self, cols, tol=None, device=None, form="double"):
+        """I(q) for flat inputs: the network where its predicted error is
+        within `tol` (log I), the plain kernel elsewhere.  Returns (I, mask of
+        points that fell back)."""
+        tol = self.TOL if tol is None else tol
+        logi = self.predict_log(cols)
+        back = self.predicted_error(cols) > tol
+        I = np.exp(logi)
+        if back.any():
+            I[back] = self.plain(cols, back, device, form)
+        return I, back
+
+    def plain(self, cols, mask, device=None, form="double"):
+        """Plain-kernel I(q) (with contrast) at the masked points, one plain
+        evaluation per parameter set over just its masked q."""
+        idx = np.nonzero(mask)[0]
+        sid = cols["set"][idx]
+        order = np.argsort(sid, kind="stable")
+        idx, sid = idx[order], sid[order]
+        starts = np.flatnonzero(np.r_[True, sid[1:] != sid[:-1]])
+        ends = np.r_[starts[1:], len(sid)]
+        first = idx[starts]
+        sets = {k: cols[k][first] for k in ("radius", "length", "rpd", "lpd", "contrast",
+                                            "flag")}
+        sets["flag"] = sets["flag"].astype(int)
+        qs = [cols["q"][idx[a:b]] for a, b in zip(starts, ends)]
+        iq = plain_unit_iq(sets, qs, device or self.net.device, form)
+        vals = np.empty(len(idx))
+        for (a, b), v, c in zip(zip(starts, ends), iq, sets["contrast"]):
+            vals[a:b] = v*c*c
+        out = np.empty(len(mask))
+        out[idx] = vals
+        return out[mask]
+
+    def save(self, path):
+        st = self.net.state()
+        np.savez(path, y_mean=self.y_mean, y_std=self.y_std, table=self.table,
+                 **{"e%d" % k: e for k, e in enumerate(self.edges)},
+                 **{"W%d" % l: st["W"][l] for l in range(4)},
+                 **{"b%d" % l: st["b"][l] for l in range(4)},
+                 w_out=st["w_out"], b_out=st["b_out"])
+
+    def load(self, path):
+        d = np.load(path)
+        self.y_mean = float(d["y_mean"])
+        self.y_std = float(d["y_std"])
+        self.table = d["table"]
+        self.edges = [d["e%d" % k] for k in range(4)]
+        self.net.load_state({"W": [d["W%d" % l] for l in range(4)],
+                             "b": [d["b%d" % l] for l in range(4)],
+                             "w_out": d["w_out"], "b_out": d["b_out"]})
+
+
+def train_and_evaluate(n_train_sets=50000, nq=1000, epochs=10, n_holdout_sets=1000,
+                       batch=8192, lr=2e-3, tol=0.01, seed=0, device=None, log=None,
+                       data_form="float32c"):
+    """
+    Generate training data with the plain kernels, train the network, judge
+    it on held-out sets evaluated by the plain FP64 kernels (half calibrates
+    the error table, half measures), and time the surrogate with automatic
+    fallback against the plain FP64 path on the measured half.
+    """
+    import time
+    import torch
+    say = log or (lambda *a: None)
+    S = Surrogate(device=device, seed=seed)
+    t0 = time.perf_counter()
+    cols, y = S.dataset(n_train_sets, nq, seed + 1, form=data_form)
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    say("data: %d samples in %.1f s" % (len(y), t_data))
+    t0 = time.perf_counter()
+    losses = S.fit(cols, y, epochs=epochs, batch=batch, lr=lr, seed=seed, log=say)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    del cols, y
+    rng = np.random.default_rng(seed + 2)
+    sets = sample_sets(n_holdout_sets, rng)
+    qs = [sample_q(nq, rng) for _ in range(n_holdout_sets)]
+    half = n_holdout_sets//2
+    cal = ({k: v[:half] for k, v in sets.items()}, qs[:half])
+    ev = ({k: v[half:] for k, v in sets.items()}, qs[half:])
+    cal_cols = flatten(*cal)
+    cal_y = np.log(np.concatenate(plain_unit_iq(cal[0], cal[1], S.net.device, "double")))
+    S.calibrate(cal_cols, cal_y)
+    ev_cols = flatten(*ev)
+    # plain FP64 path on the measured half (also the ground truth)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ev_iq = plain_unit_iq(ev[0], ev[1], S.net.device, "double")
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    truth = np.log(np.concatenate(ev_iq)) + 2*np.log(np.abs(ev_cols["contrast"]))
+    S.predict_log(ev_cols)            # warm
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    S.predict_log(ev_cols)
+    torch.cuda.synchronize()
+    t_net = time.perf_counter() - t0
+    raw = np.abs(S.predict_log(ev_cols) - truth)
+    n = len(truth)
+    report = dict(
+        train_samples=int(n_train_sets*nq), epochs=epochs, data_s=t_data, train_s=t_train,
+        final_loss=losses[-1], holdout_samples=int(n),
+        net_median_err=float(np.median(raw)), net_p90_err=float(np.quantile(raw, 0.9)),
+        net_p99_err=float(np.quantile(raw, 0.99)),
+        plain_samples_per_s=n/t_plain, net_only_samples_per_s=n/t_net,
+        net_only_speedup=t_plain/t_net, operating_points={})
+    # surrogate with automatic fallback, timed end to end, at each tolerance
+    for t in sorted({tol, 0.05}):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        I, back = S.iq(ev_cols, tol=t)
+        torch.cuda.synchronize()
+        t_sur = time.perf_counter() - t0
+        err = np.abs(np.log(I) - truth)
+        report["operating_points"]["%g" % t] = dict(
+            net_frac_within=float(np.mean(raw <= t)), fallback_frac=float(back.mean()),
+            frac_within=float(np.mean(err <= t)), max_err=float(err.max()),
+            samples_per_s=n/t_sur, speedup=t_plain/t_sur)
+    return S, report

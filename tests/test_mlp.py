@@ -13,7 +13,7 @@ from oracle import mlp_ref
 def _random_net(rng, scale=0.5, nin=16, hid=256):
     W = [rng.normal(0, scale/np.sqrt(nin if l == 0 else hid), (hid, nin if l == 0 else hid))
          for l in range(4)]
-    W[0][:, 7:] = 0.0
+    W[0][:, 15:] = 0.0
     b = [rng.normal(0, 0.1, hid) for _ in range(4)]
     w_out = rng.normal(0, 1/np.sqrt(hid), hid)
     return W, b, w_out, 0.3
@@ -77,11 +77,15 @@ def _gpu_net(rng):
 
 
 def _inputs(rng, n, n_pad):
+    """Features as the compensated pair the kernels take: hi, lo (device)
+    and their float64 sum (host)."""
     import torch
     x = np.zeros((n_pad, 16))
-    x[:n, :7] = rng.uniform(-1, 1, (n, 7))
-    xb = mlp_ref.bf16(x)
-    return torch.as_tensor(xb, dtype=torch.bfloat16, device="cuda"), xb
+    x[:n, :11] = rng.uniform(-1, 1, (n, 11))
+    hi = mlp_ref.bf16(x)
+    lo = mlp_ref.bf16(x - hi)
+    return (torch.as_tensor(hi, dtype=torch.bfloat16, device="cuda"),
+            torch.as_tensor(lo, dtype=torch.bfloat16, device="cuda"), hi + lo, hi)
 
 
 @pytest.mark.gpu
@@ -89,8 +93,8 @@ def test_tc_forward_matches_oracle(cuda):
     rng = np.random.default_rng(3)
     net, W, b, w_out, b_out = _gpu_net(rng)
     n, n_pad = 300, 384
-    x, xh = _inputs(rng, n, n_pad)
-    out = net.forward(x, n)
+    x, xlo, xh, _ = _inputs(rng, n, n_pad)
+    out = net.forward(x, xlo, n)
     net.stream.synchronize()
     assert net.errors() == 0
     got = out.cpu().numpy()[:n]
@@ -110,9 +114,9 @@ def test_tc_gradients_match_oracle(cuda):
     rng = np.random.default_rng(4)
     net, W, b, w_out, b_out = _gpu_net(rng)
     n, n_pad = 500, 512
-    x, xh = _inputs(rng, n, n_pad)
+    x, xlo, xh, xhi = _inputs(rng, n, n_pad)
     y = torch.as_tensor(rng.normal(0, 1, n_pad), dtype=torch.float32, device="cuda")
-    loss, dW, db, dwo, dbo = net.gradients(x, y, n)
+    loss, dW, db, dwo, dbo = net.gradients(x, xlo, y, n)
     net.stream.synchronize()
     assert net.errors() == 0
     Wf = [np.float32(w).astype(np.float64) for w in W]
@@ -122,7 +126,8 @@ def test_tc_gradients_match_oracle(cuda):
     yv = y.cpu().numpy().astype(np.float64)
     dout = np.zeros(n_pad)
     dout[:n] = 2*(out[:n] - yv[:n])/n
-    rW, rb, rwo, rbo = mlp_ref.backward(xh, Wf, wof, dout, zs, hs)
+    # the layer-0 weight gradient uses the high half of the inputs
+    rW, rb, rwo, rbo = mlp_ref.backward(xhi, Wf, wof, dout, zs, hs)
     for l in range(4):
         nb = 16 if l == 0 else 256
         g = dW[l].cpu().numpy().reshape(net.splits, 256, nb).sum(axis=0)
@@ -147,13 +152,17 @@ def test_tc_training_reduces_loss(cuda):
     xs = np.zeros((n, 16))
     xs[:, :7] = rng.uniform(-1, 1, (n, 7))
     target = np.sin(2*xs[:, 0]) + xs[:, 1]*xs[:, 5] - 0.5*xs[:, 3]**2
-    x = torch.as_tensor(xs, dtype=torch.bfloat16, device="cuda")
+    hi = mlp_ref.bf16(xs)
+    x = torch.as_tensor(hi, dtype=torch.bfloat16, device="cuda")
+    xlo = torch.as_tensor(mlp_ref.bf16(xs - hi), dtype=torch.bfloat16, device="cuda")
     y = torch.as_tensor(target, dtype=torch.float32, device="cuda")
     first = None
     for step in range(300):
-        loss = net.train_step(x, y, n, lr=2e-3)
+        loss = net.train_step(x, xlo, y, n, lr=2e-3)
         if first is None:
+            net.stream.synchronize()
             first = float(loss.item())
+    net.stream.synchronize()
     last = float(loss.item())
     assert net.errors() == 0
     assert last < first/10, (first, last)
