@@ -446,6 +446,32 @@ FLOPS_PER_EVAL = {"cylinder2d": 160.8}
 TRAFFIC_PER_STEP = {"cylinder2d": 39.36e6}
 
 
+def run_surrogate(args, world, rank, local):
+    """Learned surrogate: train on plain-kernel data, judge on held-out sets,
+    time the network with automatic fallback against the plain FP64 path."""
+    if rank != 0:
+        return
+    import torch
+    from sasmodels_b200.surrogate import train_and_evaluate
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    S, rep = train_and_evaluate(n_train_sets=args.surrogate_sets, nq=1000,
+                                epochs=args.surrogate_epochs, n_holdout_sets=1500,
+                                device=dev)
+    op = rep["operating_points"]["0.01"]
+    line = {
+        "metric": "surrogate log I(q) samples/s at <=1% log-I error with fallback",
+        "value": op["samples_per_s"], "unit": "samples/s", "n_gpus": 1,
+        "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16 (compensated activations), f32 accumulate",
+        "data": "synthetic (plain-kernel labels)",
+        "config": {"workload": "polydisperse cylinder surrogate, 7 inputs -> 4x256 SiLU -> log I",
+                   "train_samples": rep["train_samples"], "epochs": rep["epochs"]},
+        "surrogate": rep,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -453,7 +479,10 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="cylinder2d",
-                    choices=["cylinder2d", "sphere1d", "magnetic"])
+                    choices=["cylinder2d", "sphere1d", "magnetic", "surrogate"])
+    ap.add_argument("--surrogate-sets", type=int, default=50000,
+                    help="training parameter sets (x 1000 q each)")
+    ap.add_argument("--surrogate-epochs", type=int, default=16)
     ap.add_argument("--grid", type=int, default=256,
                     help="q grid edge for cylinder2d (smaller for profiling)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -466,6 +495,8 @@ def main(argv=None):
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.config == "surrogate":
+            run_surrogate(args, world, rank, local)
         else:
             run_b200(args, world, rank, local)
     finally:

@@ -13,8 +13,9 @@ its judge and its fallback.
   at theta = 90, phi = 0 without jitter, with q along qx.
 * The intensity is exactly quadratic in the contrast, so the network learns
   y = log I at unit contrast and ``2 log|contrast|`` is added back.
-* Predicted error: a calibration table of the held-out |error| (95th
-  percentile) over (log qR, log qL/2, R_pd, L_pd, flag) bins.  Points whose predicted error
+* Predicted error: a calibration table of the held-out |error| (99th
+  percentile) over bins of the oscillation the dispersity leaves at each
+  point (exp(-2 (pd * phase)^2)), its log phase and the flag.  Points whose predicted error
   exceeds the tolerance (default 1 % in log I), or that fall outside the
   training domain, are recomputed by the plain kernel.
 
@@ -259,15 +260,22 @@ class MLP:
 # data, training, calibration and inference with fallback
 # --------------------------------------------------------------------------
 
-def sample_sets(n_sets, rng, flag=None):
+def sample_sets(n_sets, rng, flag=None, low_pd_frac=0.0, low_pd_max=0.08):
     """Parameter sets drawn over the training domain (log-uniform sizes,
-    uniform polydispersities and contrast, random orientation flag)."""
+    uniform polydispersities and contrast, random orientation flag).  With
+    low_pd_frac > 0 that fraction of the sets draws its dispersities from
+    [0, low_pd_max] instead, oversampling the sharply oscillating curves the
+    network finds hardest."""
     lo, hi = DOMAIN["radius"]
     R = np.exp(rng.uniform(np.log(lo), np.log(hi), n_sets))
     lo, hi = DOMAIN["length"]
     L = np.exp(rng.uniform(np.log(lo), np.log(hi), n_sets))
     rpd = rng.uniform(*DOMAIN["rpd"], n_sets)
     lpd = rng.uniform(*DOMAIN["lpd"], n_sets)
+    if low_pd_frac > 0:
+        low = rng.uniform(0, 1, n_sets) < low_pd_frac
+        rpd[low] = rng.uniform(0, low_pd_max, low.sum())
+        lpd[low] = rng.uniform(0, low_pd_max, low.sum())
     contrast = rng.uniform(*DOMAIN["contrast"], n_sets)
     f = rng.integers(0, 2, n_sets) if flag is None else np.full(n_sets, flag)
     return dict(radius=R, length=L, rpd=rpd, lpd=lpd, contrast=contrast, flag=f)
@@ -348,9 +356,9 @@ class Surrogate:
         self.edges = None
 
     # ---- data --------------------------------------------------------------
-    def dataset(self, n_sets, nq, seed, form="float32c"):
+    def dataset(self, n_sets, nq, seed, form="float32c", low_pd_frac=0.0):
         rng = np.random.default_rng(seed)
-        sets = sample_sets(n_sets, rng)
+        sets = sample_sets(n_sets, rng, low_pd_frac=low_pd_frac)
         qs = [sample_q(nq, rng) for _ in range(n_sets)]
         iq = plain_unit_iq(sets, qs, self.net.device, form)
         cols = flatten(sets, qs)
@@ -411,26 +419,37 @@ class Surrogate:
         logc = 2.0*np.log(np.abs(cols["contrast"]))
         return out.cpu().numpy() + logc
 
+    @staticmethod
+    def hardness(cols):
+        """Oscillation left after dispersity damping at each point: the
+        cross-section term exp(-2 (R_pd qR)^2) for the orientation average,
+        the length term exp(-2 (L_pd qL/2)^2) for the oriented case; and the
+        log phase (qR or qL/2) of that term."""
+        qr = cols["q"]*cols["radius"]
+        qh = 0.5*cols["q"]*cols["length"]
+        flag = cols["flag"].astype(bool)
+        amp = np.where(flag, np.exp(-2*(cols["rpd"]*qr)**2), np.exp(-2*(cols["lpd"]*qh)**2))
+        phase = np.log(np.where(flag, qr, qh))
+        return amp, phase
+
     def _bins(self, cols):
-        """Calibration bin of each point: log(qR), log(qL/2), R_pd, L_pd,
-        flag -- the quantities the network's error follows."""
-        vals = (np.log(cols["q"]*cols["radius"]), np.log(0.5*cols["q"]*cols["length"]),
-                cols["rpd"], cols["lpd"])
+        amp, phase = self.hardness(cols)
+        vals = (amp, phase)
         k = [np.clip(np.searchsorted(e, v) - 1, 0, len(e) - 2)
              for e, v in zip(self.edges, vals)]
         return tuple(k) + (cols["flag"].astype(int),)
 
-    def calibrate(self, cols, y_true, quantile=0.95, nbins=(14, 14, 4, 4), min_count=25):
-        """Error table: the `quantile` of |log I error| per bin of a
-        held-out set judged by the plain kernel; bins with fewer than
-        `min_count` points predict infinity (always fall back)."""
+    def calibrate(self, cols, y_true, quantile=0.99, nbins=(16, 24), min_count=50):
+        """Error table: the `quantile` of |log I error| per (oscillation
+        amplitude, log phase, flag) bin of a held-out set judged by the plain
+        kernel; bins with fewer than `min_count` points predict infinity
+        (always fall back)."""
         pred = self.predict_log(cols) - 2.0*np.log(np.abs(cols["contrast"]))
         err = np.abs(pred - y_true)
         q0, q1 = DOMAIN["q"]
-        lims = [(np.log(q0*DOMAIN["radius"][0]), np.log(q1*DOMAIN["radius"][1])),
-                (np.log(0.5*q0*DOMAIN["length"][0]), np.log(0.5*q1*DOMAIN["length"][1])),
-                DOMAIN["rpd"], DOMAIN["lpd"]]
-        self.edges = [np.linspace(lo, hi, nb + 1) for (lo, hi), nb in zip(lims, nbins)]
+        lo = min(np.log(q0*DOMAIN["radius"][0]), np.log(0.5*q0*DOMAIN["length"][0]))
+        hi = max(np.log(q1*DOMAIN["radius"][1]), np.log(0.5*q1*DOMAIN["length"][1]))
+        self.edges = [np.linspace(0.0, 1.0, nbins[0] + 1), np.linspace(lo, hi, nbins[1] + 1)]
         keys = self._bins(cols)
         shape = tuple(nbins) + (2,)
         flat = np.ravel_multi_index(keys, shape)
@@ -454,10 +473,11 @@ class Surrogate:
         pe = self.table[self._bins(cols)]
         return np.where(inside, pe, np.inf)
 
-    def iq(self, cols, tol=None, device=None, form="double"):
+    def iq(self, cols, tol=None, device=None, form="float32c"):
         """I(q) for flat inputs: the network where its predicted error is
-        within `tol` (log I), the plain kernel elsewhere.  Returns (I, mask of
-        points that fell back)."""
+        within `tol` (log I), the plain kernel elsewhere (its FP32c form by
+        default, within 1e-5 of FP64, far inside the tolerance).  Returns
+        (I, mask of points that fell back)."""
         tol = self.TOL if tol is None else tol
         logi = self.predict_log(cols)
         back = self.predicted_error(cols) > tol
@@ -501,7 +521,7 @@ class Surrogate:
         self.y_mean = float(d["y_mean"])
         self.y_std = float(d["y_std"])
         self.table = d["table"]
-        self.edges = [d["e%d" % k] for k in range(4)]
+        self.edges = [d["e%d" % k] for k in range(len(d["table"].shape) - 1)]
         self.net.load_state({"W": [d["W%d" % l] for l in range(4)],
                              "b": [d["b%d" % l] for l in range(4)],
                              "w_out": d["w_out"], "b_out": d["b_out"]})
@@ -509,7 +529,7 @@ class Surrogate:
 
 def train_and_evaluate(n_train_sets=50000, nq=1000, epochs=10, n_holdout_sets=1000,
                        batch=8192, lr=2e-3, tol=0.01, seed=0, device=None, log=None,
-                       data_form="float32c"):
+                       data_form="float32c", low_pd_frac=0.4):
     """
     Generate training data with the plain kernels, train the network, judge
     it on held-out sets evaluated by the plain FP64 kernels (half calibrates
@@ -521,7 +541,7 @@ def train_and_evaluate(n_train_sets=50000, nq=1000, epochs=10, n_holdout_sets=10
     say = log or (lambda *a: None)
     S = Surrogate(device=device, seed=seed)
     t0 = time.perf_counter()
-    cols, y = S.dataset(n_train_sets, nq, seed + 1, form=data_form)
+    cols, y = S.dataset(n_train_sets, nq, seed + 1, form=data_form, low_pd_frac=low_pd_frac)
     torch.cuda.synchronize()
     t_data = time.perf_counter() - t0
     say("data: %d samples in %.1f s" % (len(y), t_data))
@@ -533,19 +553,24 @@ def train_and_evaluate(n_train_sets=50000, nq=1000, epochs=10, n_holdout_sets=10
     rng = np.random.default_rng(seed + 2)
     sets = sample_sets(n_holdout_sets, rng)
     qs = [sample_q(nq, rng) for _ in range(n_holdout_sets)]
-    half = n_holdout_sets//2
+    half = (2*n_holdout_sets)//3
     cal = ({k: v[:half] for k, v in sets.items()}, qs[:half])
     ev = ({k: v[half:] for k, v in sets.items()}, qs[half:])
     cal_cols = flatten(*cal)
     cal_y = np.log(np.concatenate(plain_unit_iq(cal[0], cal[1], S.net.device, "double")))
     S.calibrate(cal_cols, cal_y)
     ev_cols = flatten(*ev)
-    # plain FP64 path on the measured half (also the ground truth)
+    # plain FP64 path on the measured part (also the ground truth), and the
+    # plain FP32c path for reference
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     ev_iq = plain_unit_iq(ev[0], ev[1], S.net.device, "double")
     torch.cuda.synchronize()
     t_plain = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    plain_unit_iq(ev[0], ev[1], S.net.device, "float32c")
+    torch.cuda.synchronize()
+    t_plain32 = time.perf_counter() - t0
     truth = np.log(np.concatenate(ev_iq)) + 2*np.log(np.abs(ev_cols["contrast"]))
     S.predict_log(ev_cols)            # warm
     torch.cuda.synchronize()
@@ -560,9 +585,12 @@ def train_and_evaluate(n_train_sets=50000, nq=1000, epochs=10, n_holdout_sets=10
         final_loss=losses[-1], holdout_samples=int(n),
         net_median_err=float(np.median(raw)), net_p90_err=float(np.quantile(raw, 0.9)),
         net_p99_err=float(np.quantile(raw, 0.99)),
-        plain_samples_per_s=n/t_plain, net_only_samples_per_s=n/t_net,
+        plain_samples_per_s=n/t_plain, plain_f32c_samples_per_s=n/t_plain32,
+        net_only_samples_per_s=n/t_net,
         net_only_speedup=t_plain/t_net, operating_points={})
     # surrogate with automatic fallback, timed end to end, at each tolerance
+    # (one untimed call first so the fallback engine is loaded)
+    S.iq({k: v[:2000] for k, v in ev_cols.items()}, tol=tol)
     for t in sorted({tol, 0.05}):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -573,5 +601,6 @@ def train_and_evaluate(n_train_sets=50000, nq=1000, epochs=10, n_holdout_sets=10
         report["operating_points"]["%g" % t] = dict(
             net_frac_within=float(np.mean(raw <= t)), fallback_frac=float(back.mean()),
             frac_within=float(np.mean(err <= t)), max_err=float(err.max()),
-            samples_per_s=n/t_sur, speedup=t_plain/t_sur)
+            samples_per_s=n/t_sur, speedup=t_plain/t_sur,
+            speedup_vs_plain_f32c=t_plain32/t_sur)
     return S, report
