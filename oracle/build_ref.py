@@ -75,13 +75,35 @@ def build(models, sasmodels_path=DEFAULT_SASMODELS, force=False):
     return built
 
 
+def c_models(sasmodels_path=DEFAULT_SASMODELS):
+    """Every model plugin with C sources that loads here."""
+    if sasmodels_path not in sys.path:
+        sys.path.insert(0, sasmodels_path)
+    os.environ.setdefault("SAS_OPENCL", "none")
+    from sasmodels import core
+    models_dir = os.path.join(os.path.dirname(core.__file__), "models")
+    out = []
+    for f in sorted(os.listdir(models_dir)):
+        if not f.endswith(".py") or f.startswith("_"):
+            continue
+        try:
+            info = core.load_model_info(f[:-3])
+        except Exception:
+            continue
+        if info.source or getattr(info, "c_code", None):
+            out.append(f[:-3])
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("models", nargs="*")
     ap.add_argument("--sasmodels", default=DEFAULT_SASMODELS)
+    ap.add_argument("--all", action="store_true", help="every C model plugin")
     ap.add_argument("--force", action="store_true")
     args = ap.parse_args(argv)
-    for so in build(args.models or DEFAULT_MODELS, args.sasmodels, args.force):
+    models = c_models(args.sasmodels) if args.all else (args.models or DEFAULT_MODELS)
+    for so in build(models, args.sasmodels, args.force):
         print(so)
 
 

@@ -163,16 +163,37 @@ def build(models=None, jobs=None, force=False, verbose=False, sasmodels_path=Non
     return [os.path.join(LIB, "libsasb200_%s.so" % m) for m in models] + support
 
 
+def c_models():
+    """Every model plugin with C sources that loads in the imported sasmodels."""
+    from sasmodels import core
+    models_dir = os.path.join(os.path.dirname(core.__file__), "models")
+    out = []
+    for f in sorted(os.listdir(models_dir)):
+        if not f.endswith(".py") or f.startswith("_"):
+            continue
+        try:
+            info = core.load_model_info(f[:-3])
+        except Exception:
+            continue
+        if info.source or getattr(info, "c_code", None):
+            out.append(f[:-3])
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("models", nargs="*")
+    ap.add_argument("--all", action="store_true", help="every C model plugin")
     ap.add_argument("--sasmodels", default=None)
     ap.add_argument("--jobs", type=int, default=None)
     ap.add_argument("--force", action="store_true")
     ap.add_argument("-v", "--verbose", action="store_true")
     args = ap.parse_args(argv)
-    for so in build(args.models or None, args.jobs, args.force, args.verbose,
-                    args.sasmodels):
+    models = args.models or None
+    if args.all:
+        import_sasmodels(args.sasmodels)
+        models = c_models()
+    for so in build(models, args.jobs, args.force, args.verbose, args.sasmodels):
         print(so)
 
 

@@ -115,7 +115,20 @@ __host__ void launch_main(dim3 grid, cudaStream_t st, int nq, const double *q,
                           const double *values, const double *table,
                           const int *counts, int nseg, double *partial)
 {
-    iq_main<M, VAR, LQ, WARPS><<<grid, 32*WARPS, 0, st>>>(
+    // the staged segment is dynamic shared memory: SEG rows of the table
+    constexpr size_t stage = (size_t)SEG*Layout<M, VAR>::NF*sizeof(double);
+    if (stage > 48*1024) {
+        // the opt-in limit is per device; setting it again is harmless
+        static int raised[64] = {};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 0 || dev >= 64 || !raised[dev]) {
+            cudaFuncSetAttribute(iq_main<M, VAR, LQ, WARPS>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
+            if (dev >= 0 && dev < 64) raised[dev] = 1;
+        }
+    }
+    iq_main<M, VAR, LQ, WARPS><<<grid, 32*WARPS, stage, st>>>(
         nq, q, values, table, counts, nseg, partial);
 }
 

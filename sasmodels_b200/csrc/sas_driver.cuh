@@ -346,7 +346,7 @@ iq_main(int nq, const double *__restrict__ q, const double *__restrict__ values,
     constexpr bool MAG = (VAR == VAR_IMAGNETIC) && (M::NMAG > 0);
     constexpr int NMAGS = M::NMAG > 0 ? M::NMAG : 1;
 
-    __shared__ __align__(16) double stage[SEG*NF];
+    extern __shared__ __align__(16) double stage[];     // SEG*NF doubles (dynamic)
     __shared__ double red[WARPS][LQ][L::NOUT];
 
     const int lane = threadIdx.x & 31;

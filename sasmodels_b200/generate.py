@@ -187,10 +187,14 @@ def _param_slots(table):
 
 
 def _arg_refs(pars, slots, vec="v"):
+    """Call arguments for *pars*: a scalar slot, or for a vector parameter a
+    pointer to its first slot (plugins declare these `double p[]`; they only
+    read them)."""
     refs = []
     for p in pars:
         off, n = slots[p.id]
-        refs.append("%s[%d]" % (vec, off) if n == 1 else "(%s+%d)" % (vec, off))
+        refs.append("%s[%d]" % (vec, off) if n == 1
+                    else "const_cast<double *>(%s + %d)" % (vec, off))
     return refs
 
 

@@ -12,7 +12,10 @@ Writes, per model, ``<model>.json`` holding
   values vector and the magnetic flag produced by the reference's
   ``direct_model.get_mesh`` + ``details.make_kernel_args``;
 * ``dll``: raw result vectors of the reference DLL (``kerneldll.DllKernel``)
-  on seeded inputs, used to pin ``oracle/`` without the reference present.
+  on seeded inputs, used to pin ``oracle/`` without the reference present;
+
+and ``models_all.json``: for every C model plugin, its embedded test cases
+with the reference DLL's raw result vector on each.
 
 Run where the reference source tree is importable; the tests read only the
 JSON output.
@@ -115,9 +118,62 @@ def marshal_cases(name):
     return cases
 
 
+def c_models():
+    """Every model plugin with C sources that loads here."""
+    from sasmodels import core
+    models_dir = os.path.join(os.path.dirname(core.__file__), "models")
+    out = []
+    for f in sorted(os.listdir(models_dir)):
+        if not f.endswith(".py") or f.startswith("_"):
+            continue
+        name = f[:-3]
+        try:
+            info = core.load_model_info(name)
+        except Exception:
+            continue
+        if info.source or getattr(info, "c_code", None):
+            out.append(name)
+    return out
+
+
+def all_models_record():
+    """Embedded tests of every C model, with the reference DLL's raw result
+    for each case (tests/golden/models_all.json)."""
+    from sasmodels import core, direct_model
+    from sasmodels.details import make_kernel_args
+    from sasmodels.product import RADIUS_MODE_ID
+    record = {}
+    for name in c_models():
+        info = core.load_model_info(name)
+        model = core.build_model(info, dtype="double", platform="dll")
+        cases = []
+        for case in model_tests(info):
+            qv = [np.asarray(v, 'd') for v in case["q"]]
+            pars = dict(case["pars"])
+            pars.pop(RADIUS_MODE_ID, None)
+            try:
+                kernel = model.make_kernel(qv)
+                mesh = direct_model.get_mesh(info, pars, dim=kernel.dim)
+                details, values, magnetic = make_kernel_args(kernel, mesh)
+                kernel._call_kernel(details, values, 0., magnetic, 0)
+            except Exception:
+                continue
+            nout = 2 if info.have_Fq and case["dim"] == "1d" else 1
+            nq = len(qv[0])
+            case["raw"] = kernel.result[:nout*nq].tolist() + \
+                kernel.result[nout*nq:nout*nq + 4].tolist()
+            case["magnetic"] = bool(magnetic)
+            cases.append(case)
+        record[name] = cases
+        print(name, len(cases), "cases")
+    with open(os.path.join(HERE, "models_all.json"), "w") as fid:
+        json.dump(record, fid, indent=0)
+
+
 def main():
     from sasmodels import core, direct_model
     from sasmodels.details import make_kernel_args
+    all_models_record()
     for name in MODELS:
         info = core.load_model_info(name)
         model = core.build_model(info, dtype="double", platform="dll")
