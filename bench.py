@@ -446,6 +446,26 @@ FLOPS_PER_EVAL = {"cylinder2d": 160.8}
 TRAFFIC_PER_STEP = {"cylinder2d": 39.36e6}
 
 
+def run_population(args, world, rank, local):
+    """Fit population: batched FP32c persistent launch vs plain FP64 per-set
+    launches on every `--pop-stride`-th set of the 4096-set population."""
+    if rank != 0:
+        return
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    rep = population_compare(4096, args.pop_stride, dev)
+    line = {
+        "metric": METRIC, "value": rep["batched_f32c_sets_per_s"], "unit": "param-sets/s",
+        "n_gpus": 1, "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 compensated (f64 phases and sums)",
+        "data": "synthetic", "config": {"workload": "ellipsoid + core_shell_cylinder 1D population",
+                                        "sample": rep["sample"]},
+        "population": rep,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_surrogate(args, world, rank, local):
     """Learned surrogate: train on plain-kernel data, judge on held-out sets,
     time the network with automatic fallback against the plain FP64 path."""
@@ -456,8 +476,8 @@ def run_surrogate(args, world, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     S, rep = train_and_evaluate(n_train_sets=args.surrogate_sets, nq=1000,
-                                epochs=args.surrogate_epochs, n_holdout_sets=1500,
-                                device=dev)
+                                epochs=args.surrogate_epochs,
+                                n_holdout_sets=args.surrogate_holdout, device=dev)
     op = rep["operating_points"]["0.01"]
     line = {
         "metric": "surrogate log I(q) samples/s at <=1% log-I error with fallback",
@@ -479,7 +499,10 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="cylinder2d",
-                    choices=["cylinder2d", "sphere1d", "magnetic", "surrogate"])
+                    choices=["cylinder2d", "sphere1d", "magnetic", "surrogate", "population"])
+    ap.add_argument("--pop-stride", type=int, default=7,
+                    help="population config: evaluate every n-th of the 4096 sets")
+    ap.add_argument("--surrogate-holdout", type=int, default=1500)
     ap.add_argument("--surrogate-sets", type=int, default=50000,
                     help="training parameter sets (x 1000 q each)")
     ap.add_argument("--surrogate-epochs", type=int, default=16)
@@ -497,6 +520,8 @@ def main(argv=None):
             run_reference(args, world, rank)
         elif args.config == "surrogate":
             run_surrogate(args, world, rank, local)
+        elif args.config == "population":
+            run_population(args, world, rank, local)
         else:
             run_b200(args, world, rank, local)
     finally:

@@ -1,0 +1,126 @@
+"""
+One process per GPU (torch.distributed) for the two ways the path shards:
+
+* a fit population: independent parameter sets, split across ranks by
+  estimated cost (longest first onto the least-loaded rank), evaluated
+  locally, curves gathered back in the caller's order;
+* one large detector image: q points split into contiguous blocks, every
+  rank integrating the same dispersity mesh, the blocks gathered back (the
+  four norm sums are identical on every rank, so rank 0's are kept).
+
+Neither needs a reduction on the data path -- the only collective is the
+final gather of results.  The evaluation itself is a callable, the GPU
+engine by default, so the host logic here runs (and is tested) with the
+gloo backend on CPU as well as NCCL on GPUs.
+"""
+
+import numpy as np
+
+
+def _dist():
+    import torch.distributed as dist
+    return dist
+
+
+def world():
+    dist = _dist()
+    if dist.is_available() and dist.is_initialized():
+        return dist.get_world_size(), dist.get_rank()
+    return 1, 0
+
+
+def shard_by_cost(costs, nranks):
+    """Assignment of items to ranks: longest-processing-time-first onto the
+    least loaded rank.  Deterministic; returns a list of index lists, each in
+    increasing order."""
+    costs = np.asarray(costs, dtype=float)
+    order = np.argsort(-costs, kind="stable")
+    load = np.zeros(nranks)
+    parts = [[] for _ in range(nranks)]
+    for i in order:
+        r = int(np.argmin(load))
+        parts[r].append(int(i))
+        load[r] += costs[i]
+    return [sorted(p) for p in parts]
+
+
+def population_cost(model, sets):
+    """Relative cost of each (q, pars) set: q points x mesh points x Gauss
+    rule length at the distribution centres."""
+    from .batch import _rmax, rule_points
+    from .core import load_model_info
+    from .direct_model import make_call_args
+    info = load_model_info(model)
+    costs = []
+    for q, pars in sets:
+        q = np.asarray(q, 'd')
+        details, _, _ = make_call_args(info, pars, [q])
+        rmax = _rmax(model, pars, info)
+        pts = rule_points(q*rmax) if rmax > 0 else np.ones(q.size)
+        costs.append(float(details.num_eval*pts.sum()))
+    return costs
+
+
+def gather_in_order(local, indices, total):
+    """All-gather per-item results; returns the full list in item order on
+    every rank."""
+    dist = _dist()
+    size, _ = world()
+    if size == 1:
+        out = [None]*total
+        for i, v in zip(indices, local):
+            out[i] = v
+        return out
+    pieces = [None]*size
+    dist.all_gather_object(pieces, (list(indices), list(local)))
+    out = [None]*total
+    for idx, vals in pieces:
+        for i, v in zip(idx, vals):
+            out[i] = v
+    return out
+
+
+def evaluate_population(model, sets, evaluate=None, costs=None, **kwargs):
+    """I(q) of every set of a population, sharded over the process group.
+
+    *evaluate(model, subset)* returns the list of I(q) arrays of a subset;
+    by default the batched GPU engine on this rank's device."""
+    size, rank = world()
+    if costs is None:
+        costs = population_cost(model, sets)
+    parts = shard_by_cost(costs, size)
+    mine = parts[rank]
+    if evaluate is None:
+        evaluate = _evaluate_batched
+    local = evaluate(model, [sets[i] for i in mine], **kwargs) if mine else []
+    return gather_in_order(local, mine, len(sets))
+
+
+def _evaluate_batched(model, subset, form="float32c", device=None):
+    from .batch import Population
+    pop = Population(model, subset, form=form, device=device)
+    pop.run()
+    return pop.iq()
+
+
+def q_blocks(nq, nranks):
+    """Contiguous [lo, hi) q ranges, one per rank."""
+    b = np.linspace(0, nq, nranks + 1).astype(int)
+    return [(int(b[r]), int(b[r + 1])) for r in range(nranks)]
+
+
+def evaluate_image(q_vectors, evaluate):
+    """One image split by q blocks: *evaluate(q_block_vectors)* returns the
+    raw result (F^2 slots then the 4 norms) of its block; returns the full
+    raw vector (q slots in caller order, norms of rank 0) on every rank."""
+    size, rank = world()
+    nq = len(q_vectors[0])
+    lo, hi = q_blocks(nq, size)[rank]
+    raw = np.asarray(evaluate([np.asarray(v)[lo:hi] for v in q_vectors]))
+    nout = (len(raw) - 4)//max(hi - lo, 1) if hi > lo else 1
+    pieces = gather_in_order([raw], [rank], size)
+    out = []
+    for r, piece in enumerate(pieces):
+        a, b = q_blocks(nq, size)[r]
+        out.append(piece[:nout*(b - a)])
+    return np.concatenate(out + [pieces[0][-4:]])
