@@ -32,6 +32,17 @@ CORE_MODELS = ["sphere", "cylinder", "core_shell_sphere", "ellipsoid",
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
+#: models compiled without FMA contraction (``--fmad=false``), so that every
+#: multiply and add rounds separately as in the x86-64 reference build (gcc
+#: -O2 on baseline x86-64 has no FMA instruction to contract into).  These
+#: are the ill-conditioned ones: lattice sums near the Bragg condition
+#: (the paracrystals), the partial structure factors of a binary mixture,
+#: and the iterative Hayter-Penfold MSA solve; with contraction their F^2
+#: moves by 4e-10 .. 4e-9 relative, without it by <= 1.4e-11.  Every other
+#: model meets 1e-12 with contraction and keeps the faster DFMA form.
+STRICT_FP_MODELS = {"bcc_paracrystal", "fcc_paracrystal", "sc_paracrystal",
+                    "binary_hard_sphere", "hayter_msa"}
+
 
 def nvcc():
     path = shutil.which("nvcc")
@@ -76,7 +87,9 @@ def build_model(name, force=False, verbose=False, extra_flags=()):
     from sasmodels import core
     sm_info = core.load_model_info(name)
     src, meta = generate.make_cuda_source(sm_info, model_sources(sm_info))
-    flags = nvcc_flags(extra_flags)
+    strict = name in STRICT_FP_MODELS
+    flags = nvcc_flags((["--fmad=false"] if strict else []) + list(extra_flags))
+    meta["strict_fp"] = strict
     tag = generate.source_tag(src + " ".join(flags)
                               + _read(os.path.join(CSRC, "sas_driver.cuh"))
                               + _read(os.path.join(CSRC, "sas_abi.cuh"))
