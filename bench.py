@@ -361,7 +361,7 @@ def single_config(name, qv, pars, dtype, reps, dev):
     return len(qv[0])*details.num_eval/t, t
 
 
-def population_compare(n_sets, stride, dev):
+def population_compare(n_sets, stride, dev, tune=True):
     """Batched FP32c vs plain FP64 per-set launches on every `stride`-th set
     of the seeded population: param-sets/s of both and the max relative
     error of the batched I(q) against the FP64 plain results."""
@@ -377,7 +377,7 @@ def population_compare(n_sets, stride, dev):
     tuned = {}
     for name, members in by.items():
         sets = [(q, p) for _, q, p in members]
-        warps, ipw = autotune.tune_population(name, sets, "float32c")
+        warps, ipw = autotune.tune_population(name, sets, "float32c") if tune else (8, 8)
         tuned[name] = [warps, ipw]
         P = Population(name, sets, form="float32c", device=dev, warps=warps,
                        items_per_warp=ipw)
@@ -454,7 +454,7 @@ def run_population(args, world, rank, local):
     import torch
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    rep = population_compare(4096, args.pop_stride, dev)
+    rep = population_compare(4096, args.pop_stride, dev, tune=not args.no_tune)
     line = {
         "metric": METRIC, "value": rep["batched_f32c_sets_per_s"], "unit": "param-sets/s",
         "n_gpus": 1, "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak",

@@ -10,6 +10,10 @@ iterations of a DREAM fit) replay without launch overhead.
     pop.update([pars1b, ...])   # new values, same q and pd sizes
     pop.replay()                # graph replay
 
+``line=True`` evaluates instead the 2D kernel along the qx axis (qy = 0) at
+each set's own view angles (theta, phi), without orientation dispersion:
+the line cut of an oriented 2D pattern, for models with an Iqac kernel.
+
 The packing uses the same marshaling as a single call (``details`` and
 ``values`` per set, ``details.py:225-254``), concatenated.  Work items
 (set, 32-q tile, mesh range) are sized by a cost model of the adaptive
@@ -29,6 +33,7 @@ from .direct_model import make_call_args
 SET_FIELDS = 8
 ITEM_FIELDS = 4
 FORMS = {"double": 0, "float32c": 1}
+LINE_FORMS = {"double": 2, "float32c": 3}
 
 # warp-cycles per rule point in each mode, and fixed costs (arbitrary units;
 # only ratios matter for splitting)
@@ -57,6 +62,20 @@ def rule_points(qr):
     return np.where(qr < 10, 20, np.where(qr < 100, 76, np.where(qr < 750, 500, 5000)))
 
 
+def line_call_args(info, pars, q):
+    """(details, values) of one line-form set: marshaled as a 2D call at
+    (q, 0); orientation dispersion is refused (the line form has no jitter
+    rotation)."""
+    q = np.asarray(q, 'd')
+    details, values, _ = make_call_args(info, pars, [q, np.zeros_like(q)])
+    kpars = info.parameters.kernel_parameters
+    for d in range(details.num_active):
+        p = kpars[int(details.pd_par[d])]
+        if p.type == "orientation" and details.pd_length[d] > 1:
+            raise ValueError("line form: %s has orientation dispersion" % p.name)
+    return details, values
+
+
 def _batch_fn(model):
     lib = ct.CDLL(_abi.library_path(model))
     fn = getattr(lib, "sasb200_%s_batch" % model)
@@ -72,14 +91,21 @@ class Population:
     """A packed population of one model on one GPU (see module doc)."""
 
     def __init__(self, model, sets, form="float32c", device=None, cutoff=0.0,
-                 reff_mode=0, warps=8, blocks=0, items_per_warp=8):
+                 reff_mode=0, warps=8, blocks=0, items_per_warp=8, line=False):
         import torch
         self.torch = torch
         self.model = model
         self.info = load_model_info(model)
         if not self.info.raw.get("f32c"):
             raise ValueError("model %s has no batched kernels" % model)
+        if form not in FORMS:
+            raise ValueError("form must be one of %s" % sorted(FORMS))
         self.form = form
+        self.line = bool(line)
+        if self.line and self.info.xy_mode != "qac":
+            raise ValueError("line form needs a model with an Iqac kernel (%s is %s)"
+                             % (model, self.info.xy_mode))
+        self.form_code = (LINE_FORMS if self.line else FORMS)[form]
         self.cutoff = float(cutoff)
         self.reff_mode = int(reff_mode)
         self.warps = int(warps)
@@ -105,7 +131,7 @@ class Population:
         costs = []
         for q, pars in sets:
             q = np.ascontiguousarray(q, 'd').ravel()
-            details, values, _ = make_call_args(info, pars, [q])
+            details, values = self._marshal(pars, q)
             nq, n_eval = q.size, details.num_eval
             ntile = (nq + 31)//32
             desc.append([nq, q_off, det_off, val_off, n_eval, raw_off, iq_off, tile_off])
@@ -121,7 +147,7 @@ class Population:
             raw_off += 2*nq + 4
             iq_off += nq
             tile_off += ntile
-            rmax = _rmax(self.model, pars, info)
+            rmax = 0.0 if self.line else _rmax(self.model, pars, info)
             pts = rule_points(q*rmax) if rmax > 0 else np.ones(nq)
             costs.append(pts)
         self.n_sets = len(desc)
@@ -154,6 +180,12 @@ class Population:
             self.d_counter = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.desc = np.array(desc)
         self.stream.synchronize()
+
+    def _marshal(self, pars, q):
+        if not self.line:
+            details, values, _ = make_call_args(self.info, pars, [q])
+            return details, values
+        return line_call_args(self.info, pars, q)
 
     def _items(self, desc, costs):
         """Cut every (set, tile) into mesh ranges of similar cost."""
@@ -195,7 +227,7 @@ class Population:
         """Enqueue one evaluation of every set on ``self.stream``."""
         torch = self.torch
         with torch.cuda.device(self.device):
-            status = self.fn(FORMS[self.form], self.warps, self.blocks, self.n_sets,
+            status = self.fn(self.form_code, self.warps, self.blocks, self.n_sets,
                              self.d_sets.data_ptr(), self.d_q.data_ptr(),
                              self.d_det.data_ptr(), self.d_val.data_ptr(), self.n_items,
                              self.d_items.data_ptr(), self.d_tile_off.data_ptr(),
@@ -230,8 +262,7 @@ class Population:
         off = 0
         host = self.h_val.numpy()
         for k, pars in enumerate(pars_list):
-            q = np.zeros(1)
-            details, values, _ = make_call_args(self.info, pars, [q])
+            details, values = self._marshal(pars, np.zeros(1))
             if tuple(details.buffer) != self.pd_shape[k]:
                 raise ValueError("set %d changed its dispersity structure" % k)
             n = self._val_sizes[k]

@@ -49,7 +49,7 @@ struct Weights {
     const float *b_out;           // device scalar
 };
 
-__device__ __forceinline__ float silu(float z) { return z/(1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float dsilu(float z)
 {
     const float s = 1.0f/(1.0f + __expf(-z));
@@ -554,6 +554,220 @@ inline int32_t status(const char *what)
     return 0;
 }
 
+// ---------------------------------------------------------------- inference --
+// mlp_infer: the forward pass without the training planes, as a persistent,
+// pipelined kernel.  One CTA per SM walks 128-row tiles; a producer warp
+// streams the 24 weight chunks of every tile (layers 1-3, 8 chunks of
+// 256 x 32) through a 4-stage shared-memory ring with bulk copies (TMA
+// engine) that complete on mbarriers, running ahead into the next layer and
+// tile while the eight consumer warps do the epilogues; one consumer thread
+// issues the MMAs and frees each stage with tcgen05.commit.  The weights
+// come pre-arranged (mlp_pack) so every chunk is one contiguous 16 KB copy
+// that lands in the canonical K-major layout.  The arithmetic is that of
+// mlp_forward (same compensated activations, bias, SiLU, output dot).
+constexpr int KCI = 32;                          // K per streamed chunk
+constexpr int CHUNK_BYTES = HID*KCI*2;           // 16 KB
+constexpr int CHUNKS_PER_LAYER = HID/KCI;        // 8
+constexpr int CHUNKS_PER_TILE = 3*CHUNKS_PER_LAYER;
+constexpr int STAGES = 4;
+constexpr int W0_BYTES = HID*NIN*2;              // 8 KB
+constexpr int IMG_BYTES = W0_BYTES + CHUNKS_PER_TILE*CHUNK_BYTES;
+constexpr int X_BYTES = TM*NIN*2;                // 4 KB
+constexpr int INF_CONSUMERS = 256;               // 8 warps
+constexpr int INF_THREADS = INF_CONSUMERS + 32;  // + producer warp
+constexpr int INF_SMEM = 2*ACT_BYTES + STAGES*CHUNK_BYTES + W0_BYTES + 2*X_BYTES;
+
+struct InferParams {
+    const uint8_t *img;           // packed weights (mlp_pack)
+    const float *b[4];
+    const float *w_out;
+    const float *b_out;
+};
+
+// W_l [out][in] bf16 -> the chunk image: W0 as one 256 x 16 canonical tile,
+// then for l = 1..3 and c = 0..7 the 256 x 32 canonical tile of columns
+// [32c, 32c + 32).
+__global__ void mlp_pack(const __nv_bfloat16 *__restrict__ w0, const __nv_bfloat16 *__restrict__ w1,
+                         const __nv_bfloat16 *__restrict__ w2, const __nv_bfloat16 *__restrict__ w3,
+                         uint8_t *__restrict__ img)
+{
+    constexpr int G0 = HID*(NIN/8);                 // 16-byte groups of W0
+    constexpr int GL = HID*(HID/8);                 // of one hidden layer
+    for (int i = blockIdx.x*blockDim.x + threadIdx.x; i < G0 + 3*GL; i += gridDim.x*blockDim.x) {
+        if (i < G0) {
+            const int r = i/(NIN/8), k = 8*(i % (NIN/8));
+            *reinterpret_cast<uint4 *>(img + tc::kmajor_offset<HID>(r, k)) =
+                *reinterpret_cast<const uint4 *>(w0 + r*NIN + k);
+            continue;
+        }
+        const int j = i - G0, l = j/GL, rem = j % GL;
+        const int r = rem/(HID/8), k = 8*(rem % (HID/8));
+        const __nv_bfloat16 *w = l == 0 ? w1 : (l == 1 ? w2 : w3);
+        const int c = k/KCI;
+        uint8_t *dst = img + W0_BYTES + (size_t)(l*CHUNKS_PER_LAYER + c)*CHUNK_BYTES
+                     + tc::kmajor_offset<HID>(r, k - c*KCI);
+        *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(w + r*HID + k);
+    }
+}
+
+__global__ void __launch_bounds__(INF_THREADS, 1)
+mlp_infer(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
+          const __nv_bfloat16 *__restrict__ x_lo, InferParams prm, float *__restrict__ out,
+          int *__restrict__ err)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *act = smem;
+    uint8_t *act_lo = smem + ACT_BYTES;
+    uint8_t *ring = smem + 2*ACT_BYTES;
+    uint8_t *w0 = ring + STAGES*CHUNK_BYTES;
+    uint8_t *xs = w0 + W0_BYTES;
+    uint8_t *xs_lo = xs + X_BYTES;
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], acc_bar, w0_bar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ float dot_half[TM];
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int my_tiles = blockIdx.x < n_tiles ? (n_tiles - 1 - blockIdx.x)/gridDim.x + 1 : 0;
+
+    if (warp == 0) {
+        tc::tmem_alloc(&tmem_slot, HID);
+        tc::tmem_relinquish();
+    }
+    if (t == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::mbar_init(&acc_bar, 1);
+        tc::mbar_init(&w0_bar, 1);
+        tc::mbar_fence_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == INF_CONSUMERS/32) {
+        // ---- producer: one lane issues every bulk copy ----
+        if (lane == 0) {
+            bool ok = true;
+            tc::mbar_arrive_expect_tx(&w0_bar, W0_BYTES);
+            tc::bulk_load(w0, prm.img, W0_BYTES, &w0_bar);
+            const int total = my_tiles*CHUNKS_PER_TILE;
+            int i = 0;
+            for (; i < total; ++i) {
+                const int s = i % STAGES, use = i/STAGES;
+                if (use > 0 && !tc::mbar_wait(&empty[s], (uint32_t)((use - 1) & 1))) {
+                    ok = false;
+                    break;
+                }
+                tc::mbar_arrive_expect_tx(&full[s], CHUNK_BYTES);
+                tc::bulk_load(ring + s*CHUNK_BYTES,
+                              prm.img + W0_BYTES + (size_t)(i % CHUNKS_PER_TILE)*CHUNK_BYTES,
+                              CHUNK_BYTES, &full[s]);
+            }
+            // every issued copy has landed before the CTA may exit
+            for (int j = (i > STAGES ? i - STAGES : 0); j < i; ++j)
+                ok = tc::mbar_wait(&full[j % STAGES], (uint32_t)((j/STAGES) & 1)) && ok;
+            ok = tc::mbar_wait(&w0_bar, 0u) && ok;
+            if (!ok) atomicExch(err, 2);
+        }
+    } else {
+        // ---- consumers ----
+        bool ok = true;
+        uint32_t acc_phase = 0;
+        int chunk = 0;                                  // used by t == 0 only
+        const int quad = warp & 3, half = warp >> 2;
+        const int row = 32*quad + lane;                 // TMEM lane = tile row
+        const uint32_t lane_base = (uint32_t)(32*quad) << 16;
+        constexpr uint32_t idesc = tc::idesc_bf16(TM, HID);
+        if (t == 0) ok = tc::mbar_wait(&w0_bar, 0u);
+        ok = tc::bar_and(1, INF_CONSUMERS, ok);
+        for (int k = 0; k < my_tiles && ok; ++k) {
+            const int row0 = (blockIdx.x + k*gridDim.x)*TM;
+            {
+                const int r = t >> 1, c = (t & 1)*8;
+                const size_t g = (size_t)(row0 + r)*NIN + c;
+                *reinterpret_cast<uint4 *>(xs + tc::kmajor_offset<TM>(r, c)) =
+                    *reinterpret_cast<const uint4 *>(x + g);
+                *reinterpret_cast<uint4 *>(xs_lo + tc::kmajor_offset<TM>(r, c)) =
+                    *reinterpret_cast<const uint4 *>(x_lo + g);
+            }
+            tc::fence_async_smem();
+            tc::fence_before_sync();
+            ok = tc::bar_and(1, INF_CONSUMERS, ok);
+            tc::fence_after_sync();
+            if (!ok) break;
+            if (t == 0) {
+                const uint64_t bdesc = tc::kmajor_desc<HID>(tc::smem_u32(w0), 0);
+                tc::mma_bf16(tmem, tc::kmajor_desc<TM>(tc::smem_u32(xs), 0), bdesc, idesc, 0u);
+                tc::mma_bf16(tmem, tc::kmajor_desc<TM>(tc::smem_u32(xs_lo), 0), bdesc, idesc, 1u);
+                tc::mma_commit(&acc_bar);
+            }
+            for (int l = 0; l < 4; ++l) {
+                if (l > 0 && t == 0) {
+                    const uint32_t a_hi = tc::smem_u32(act), a_lo = tc::smem_u32(act_lo);
+                    for (int c = 0; c < CHUNKS_PER_LAYER; ++c, ++chunk) {
+                        const int s = chunk % STAGES;
+                        if (!tc::mbar_wait(&full[s], (uint32_t)((chunk/STAGES) & 1))) {
+                            ok = false;
+                            break;
+                        }
+                        tc::fence_after_sync();
+                        const uint32_t b_addr = tc::smem_u32(ring + s*CHUNK_BYTES);
+                        #pragma unroll
+                        for (int st = 0; st < KCI/16; ++st) {
+                            const uint64_t bdesc = tc::kmajor_desc<HID>(b_addr, st);
+                            const int as = c*(KCI/16) + st;
+                            tc::mma_bf16(tmem, tc::kmajor_desc<TM>(a_hi, as), bdesc, idesc,
+                                         (c > 0 || st > 0) ? 1u : 0u);
+                            tc::mma_bf16(tmem, tc::kmajor_desc<TM>(a_lo, as), bdesc, idesc, 1u);
+                        }
+                        tc::mma_commit(&empty[s]);
+                    }
+                    tc::mma_commit(&acc_bar);
+                }
+                const bool done = tc::mbar_wait(&acc_bar, acc_phase);
+                acc_phase ^= 1u;
+                tc::fence_after_sync();
+                ok = tc::bar_and(1, INF_CONSUMERS, ok && done);
+                if (!ok) break;
+                // epilogue: this thread's row, columns [128 half, 128 half + 128)
+                const float *bias = prm.b[l];
+                float dot = 0.0f;
+                #pragma unroll 1
+                for (int c0 = 128*half; c0 < 128*half + 128; c0 += 16) {
+                    uint32_t r16[16];
+                    tc::tmem_ld16(tmem + lane_base + (uint32_t)c0, r16);
+                    tc::tmem_wait_ld();
+                    float h[16];
+                    #pragma unroll
+                    for (int j = 0; j < 16; ++j) h[j] = silu(__uint_as_float(r16[j]) + bias[c0 + j]);
+                    if (l == 3) {
+                        #pragma unroll
+                        for (int j = 0; j < 16; ++j) dot = fmaf(h[j], prm.w_out[c0 + j], dot);
+                    } else {
+                        store16_split(act, act_lo, row, c0, h);
+                    }
+                }
+                if (l == 3) {
+                    if (half == 1) dot_half[row] = dot;
+                    tc::bar_sync(2, INF_CONSUMERS);
+                    if (half == 0 && row0 + row < n) out[row0 + row] = dot + dot_half[row] + *prm.b_out;
+                }
+                tc::fence_async_smem();
+                tc::fence_before_sync();
+                ok = tc::bar_and(1, INF_CONSUMERS, ok);
+                tc::fence_after_sync();
+                if (!ok) break;
+            }
+        }
+        if (!ok && t == 0) atomicExch(err, 1);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, HID);
+}
+
 }  // namespace mlp
 
 using namespace mlp;
@@ -561,6 +775,58 @@ using namespace mlp;
 extern "C" {
 
 const char *sasb200_mlp_last_error(void) { return errbuf(); }
+
+// Pack the bf16 weights [out][in] into the chunk image mlp_infer streams
+// (IMG_BYTES = 8 KB + 24 x 16 KB).
+int32_t sasb200_mlp_pack(const void *w0, const void *w1, const void *w2, const void *w3,
+                         void *img, void *stream)
+{
+    errbuf()[0] = 0;
+    if (!w0 || !w1 || !w2 || !w3 || !img)
+        return (std::snprintf(errbuf(), 256, "bad arguments"), -1);
+    mlp_pack<<<96, 256, 0, (cudaStream_t)stream>>>(
+        static_cast<const __nv_bfloat16 *>(w0), static_cast<const __nv_bfloat16 *>(w1),
+        static_cast<const __nv_bfloat16 *>(w2), static_cast<const __nv_bfloat16 *>(w3),
+        static_cast<uint8_t *>(img));
+    return status("mlp_pack");
+}
+
+int32_t sasb200_mlp_image_bytes(void) { return IMG_BYTES; }
+
+// Inference: out[n] for x, x_lo [n_pad x 16] (n_pad a multiple of 128) with
+// the packed weights; persistent grid of at most `blocks` CTAs (0 = one per
+// SM).  err receives 1 or 2 if a pipeline wait ran out.
+int32_t sasb200_mlp_infer(int32_t n, int32_t n_pad, const void *x, const void *x_lo,
+                          const void *img, const float *const *b, const float *w_out,
+                          const float *b_out, float *out, int32_t *err, int32_t blocks,
+                          void *stream)
+{
+    errbuf()[0] = 0;
+    if (n < 0 || n_pad % TM || n > n_pad || !x || !x_lo || !img || !b || !w_out || !b_out
+        || !out || !err || blocks < 0)
+        return (std::snprintf(errbuf(), 256, "bad arguments"), -1);
+    if (reinterpret_cast<uintptr_t>(img) % 16)
+        return (std::snprintf(errbuf(), 256, "weight image must be 16-byte aligned"), -1);
+    if (n_pad == 0) return 0;
+    InferParams prm;
+    prm.img = static_cast<const uint8_t *>(img);
+    for (int l = 0; l < 4; ++l) prm.b[l] = b[l];
+    prm.w_out = w_out;
+    prm.b_out = b_out;
+    const int n_tiles = n_pad/TM;
+    if (blocks == 0) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        blocks = sms > 0 ? sms : 1;
+    }
+    if (blocks > n_tiles) blocks = n_tiles;
+    cudaFuncSetAttribute(mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, INF_SMEM);
+    mlp_infer<<<blocks, INF_THREADS, INF_SMEM, (cudaStream_t)stream>>>(
+        n, n_tiles, static_cast<const __nv_bfloat16 *>(x),
+        static_cast<const __nv_bfloat16 *>(x_lo), prm, out, err);
+    return status("mlp_infer");
+}
 
 // out[n] (and z/h planes [4][n_pad x 256] when non-null) for x[n_pad x 16];
 // n_pad a multiple of 128.

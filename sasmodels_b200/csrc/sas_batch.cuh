@@ -66,6 +66,57 @@ struct QuadWhole {
     }
 };
 
+// One oriented 2D evaluation per (q, mesh point) along the qx axis (qy = 0)
+// at the set's own view angles: the line cut of a 2D pattern without
+// orientation dispersion, for models with an Iqac kernel.  The rotation and
+// the qab/qc split are those of the Iqxy kernel (mesh_prepare + eval_2d,
+// kernel_iq.c:197-242) with zero jitter, so a set gives what the 2D kernel
+// gives for q vectors (q, 0).
+template <class M>
+struct QuadLine {
+    struct S { double qab, qc; double v[M::NPARS > 0 ? M::NPARS : 1]; };
+    __device__ static S setup(double q, const double *v, const double *values)
+    {
+        S s;
+        #pragma unroll
+        for (int k = 0; k < M::NPARS; ++k) s.v[k] = v[k];
+        double rot[2];
+        rotation_ac(values[M::THETA_PAR + 2], values[M::THETA_PAR + 3],
+                    v[M::THETA_PAR], v[M::THETA_PAR + 1], rot);
+        const double qx = q, qy = 0.0;
+        s.qc = rot[0]*qx + rot[1]*qy;
+        const double qab_sq = -s.qc*s.qc + qx*qx + qy*qy;
+        s.qab = qab_sq > 0.0 ? sqrt(qab_sq) : 0.0;
+        return s;
+    }
+    __device__ static int nodes(const S &) { return 1; }
+    __device__ static void node(const S &s, int, double &, double &t2)
+    {
+        t2 += M::iqac(s.qab, s.qc, s.v);
+    }
+    __device__ static void finish(const S &, double, double t2, double &F1, double &F2)
+    {
+        F1 = 0.0;
+        F2 = t2;
+    }
+};
+
+// Q::setup(q, v, values) where the functor takes the set's values (QuadLine),
+// Q::setup(q, v) otherwise.
+template <class Q>
+__device__ __forceinline__ auto quad_setup(double q, const double *v, const double *values, int)
+    -> decltype(Q::setup(q, v, values))
+{
+    return Q::setup(q, v, values);
+}
+
+template <class Q>
+__device__ __forceinline__ typename Q::S quad_setup(double q, const double *v, const double *,
+                                                    long)
+{
+    return Q::setup(q, v);
+}
+
 // Parameters and weight of 1D mesh point `step` (same rule as mesh_prepare
 // for the Iq kernel: outermost-first weight product, VALID, cutoff).
 template <class M>
@@ -161,7 +212,7 @@ batch_main(int n_items, const int32_t *__restrict__ items, const int32_t *__rest
         for (int m = m0; m < m1; ++m) {
             double w;
             if (!mesh_point_1d<M>(det, values, m, cutoff, v, w)) continue;   // warp-uniform
-            typename Q::S s = Q::setup(qk, v);
+            typename Q::S s = quad_setup<Q>(qk, v, values, 0);
             const int n = q_ok ? Q::nodes(s) : 0;
             const bool shortq = n <= SHORT_RULE;
             if (q_ok && shortq) {
@@ -177,7 +228,7 @@ batch_main(int n_items, const int32_t *__restrict__ items, const int32_t *__rest
                 const int L = __ffs(longq) - 1;
                 longq &= longq - 1;
                 const double qL = __shfl_sync(FULL_MASK, qk, L);
-                const typename Q::S sL = Q::setup(qL, v);
+                const typename Q::S sL = quad_setup<Q>(qL, v, values, 0);
                 const int nL = Q::nodes(sL);
                 double t1 = 0.0, t2 = 0.0;
                 for (int i = lane; i < nL; i += 32) Q::node(sL, i, t1, t2);
@@ -291,12 +342,35 @@ __host__ int32_t batch_dispatch(int32_t warps, int32_t n_sets, const int32_t *se
     }
 }
 
+// Line form (QuadLine) where the model has an Iqac kernel.
+template <class M>
+__host__ int32_t batch_dispatch_line(int32_t warps, int32_t n_sets, const int32_t *sets,
+                                     const double *q_all, const int32_t *det_all,
+                                     const double *val_all, int32_t n_items,
+                                     const int32_t *items, const int32_t *tile_items_off,
+                                     const int32_t *tile_items, double cutoff,
+                                     int32_t reff_mode, double *partials, double *norms,
+                                     double *raw_all, double *iq_all, int32_t *counter,
+                                     int32_t blocks, cudaStream_t st)
+{
+    if constexpr (M::XY_MODE == XY_QAC) {
+        return batch_dispatch<M, QuadLine<M>>(warps, n_sets, sets, q_all, det_all, val_all,
+                                              n_items, items, tile_items_off, tile_items,
+                                              cutoff, reff_mode, partials, norms, raw_all,
+                                              iq_all, counter, blocks, st);
+    } else {
+        return fail(ERR_ARGUMENT, "the line form needs a model with an Iqac kernel");
+    }
+}
+
 }  // namespace sasb200
 
 // int32 sasb200_<name>_batch(form, warps, blocks, n_sets, sets, q_all, det_all,
 //     val_all, n_items, items, tile_items_off, tile_items, cutoff,
 //     reff_mode, partials, norms, raw_all, iq_all, counter, stream)
-// form 0 = FP64 (the plugin's own Fq per lane), 1 = FP32-compensated.
+// form 0 = FP64 (the plugin's own Fq per lane), 1 = FP32-compensated;
+// 2 / 3 = the line form (QuadLine: 2D along qx at the set's view angles,
+// no orientation dispersion) in FP64 / FP32-compensated.
 #define SASB200_EXPORT_BATCH(NAME, MODEL64, MODEL32)                                     \
 extern "C" int32_t sasb200_##NAME##_batch(                                              \
     int32_t form, int32_t warps, int32_t blocks, int32_t n_sets, const int32_t *sets,   \
@@ -320,5 +394,15 @@ extern "C" int32_t sasb200_##NAME##_batch(                                      
             warps, n_sets, sets, q_all, det_all, val_all, n_items, items,               \
             tile_items_off, tile_items, cutoff, reff_mode, partials, norms, raw_all,    \
             iq_all, counter, blocks, st);                                               \
-    return sasb200::fail(sasb200::ERR_ARGUMENT, "form must be 0 (FP64) or 1 (FP32c)");  \
+    if (form == 2 || form == 3)                                                         \
+        return form == 2                                                                \
+            ? sasb200::batch_dispatch_line<MODEL64>(                                    \
+                  warps, n_sets, sets, q_all, det_all, val_all, n_items, items,         \
+                  tile_items_off, tile_items, cutoff, reff_mode, partials, norms,       \
+                  raw_all, iq_all, counter, blocks, st)                                 \
+            : sasb200::batch_dispatch_line<MODEL32>(                                    \
+                  warps, n_sets, sets, q_all, det_all, val_all, n_items, items,         \
+                  tile_items_off, tile_items, cutoff, reff_mode, partials, norms,       \
+                  raw_all, iq_all, counter, blocks, st);                                \
+    return sasb200::fail(sasb200::ERR_ARGUMENT, "form must be 0..3");                   \
 }

@@ -63,6 +63,45 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
     return false;
 }
 
+// Arrive once and add `bytes` to the transaction count of the current phase
+// (the phase completes when the bulk copies have delivered that many bytes).
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// ---- bulk copy (TMA engine, untiled, no multicast) --------------------------
+// global -> this CTA's shared memory, completion counted on *bar.  Both
+// addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes,
+                                          uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
+                 " [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// ---- named barriers ----------------------------------------------------------
+// Barrier `id` among `count` threads (a multiple of 32) of the CTA.
+__device__ __forceinline__ void bar_sync(int id, int count)
+{
+    asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(count) : "memory");
+}
+
+// Barrier `id` among `count` threads that also ANDs `pred` over them.
+__device__ __forceinline__ bool bar_and(int id, int count, bool pred)
+{
+    uint32_t r;
+    asm volatile("{\n\t.reg .pred p, q;\n\t"
+                 "setp.ne.u32 p, %1, 0;\n\t"
+                 "bar.red.and.pred q, %2, %3, p;\n\t"
+                 "selp.u32 %0, 1, 0, q;\n\t}"
+                 : "=r"(r) : "r"((uint32_t)pred), "r"(id), "r"(count) : "memory");
+    return r != 0;
+}
+
 // ---- fences ----------------------------------------------------------------
 // generic-proxy shared-memory writes -> visible to the tensor-core (async) proxy
 __device__ __forceinline__ void fence_async_smem()

@@ -54,9 +54,12 @@ def _lib():
     lib.sasb200_loss_grad.argtypes = [I, I, P, P, F, P, P, P]
     lib.sasb200_adam.argtypes = [I, I, P, P, P, P, F, F, F, F, I, P, P, I, I, P]
     lib.sasb200_mlp_features.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P]
+    lib.sasb200_mlp_pack.argtypes = [P, P, P, P, P, P]
+    lib.sasb200_mlp_infer.argtypes = [I, I, P, P, P, P, P, P, P, P, I, P]
     for name in ("sasb200_mlp_forward", "sasb200_mlp_backward", "sasb200_gemm_nt",
                  "sasb200_transpose_bf16", "sasb200_row_dot", "sasb200_loss_grad",
-                 "sasb200_adam", "sasb200_mlp_features"):
+                 "sasb200_adam", "sasb200_mlp_features", "sasb200_mlp_pack",
+                 "sasb200_mlp_infer", "sasb200_mlp_image_bytes"):
         getattr(lib, name).restype = I
     lib.sasb200_mlp_last_error.restype = ct.c_char_p
     return lib
@@ -98,12 +101,17 @@ class MLP:
         #: Huber threshold of the training loss (<= 0: squared error)
         self.huber = 0.0
         self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.img = torch.empty(self.lib.sasb200_mlp_image_bytes(), dtype=torch.uint8,
+                               device=self.device)
+        self._packed = None
+        self._infer_out = None
         self._sync_bf16()
         self._scratch_n = 0
 
     # bf16 copies used by the kernels
     def _sync_bf16(self):
         torch = self.torch
+        self._wversion = getattr(self, "_wversion", 0) + 1
         self.Wb = [w.to(torch.bfloat16).contiguous() for w in self.W]
         self.WTb = [w.t().contiguous().to(torch.bfloat16) for w in self.W]
 
@@ -139,6 +147,31 @@ class MLP:
         self._scratch_n = n_pad
 
     # ----------------------------------------------------------- kernels --
+    def _pack(self):
+        """Refresh the chunked weight image of the inference kernel after the
+        bf16 weights changed (training steps, loads)."""
+        key = (self.step_count, self._wversion)
+        if self._packed == key:
+            return
+        self._check(self.lib.sasb200_mlp_pack(*[w.data_ptr() for w in self.Wb],
+                                              self.img.data_ptr(), self.stream.cuda_stream),
+                    "mlp_pack")
+        self._packed = key
+
+    def infer(self, x, x_lo, n, blocks=0):
+        """Inference only: out[n_pad] for features x + x_lo through the
+        persistent pipelined kernel (mlp_infer), on self.stream."""
+        torch = self.torch
+        n_pad = x.shape[0]
+        if self._infer_out is None or self._infer_out.numel() < n_pad:
+            self._infer_out = torch.empty(n_pad, dtype=torch.float32, device=self.device)
+        self._pack()
+        self._check(self.lib.sasb200_mlp_infer(
+            n, n_pad, x.data_ptr(), x_lo.data_ptr(), self.img.data_ptr(), self._ptrs(self.b),
+            self.w_out.data_ptr(), self.b_out.data_ptr(), self._infer_out.data_ptr(),
+            self.err.data_ptr(), int(blocks), self.stream.cuda_stream), "mlp_infer")
+        return self._infer_out[:n_pad]
+
     def forward(self, x, x_lo, n, save=False):
         """out[n_pad] for features x + x_lo (bf16 [n_pad x 16] each), on
         self.stream."""
@@ -413,7 +446,7 @@ class Surrogate:
         torch = self.torch
         x, x_lo, n = self._x(cols)
         with torch.cuda.stream(self.net.stream):
-            out = self.net.forward(x, x_lo, n)[:n].double()
+            out = self.net.infer(x, x_lo, n)[:n].double()
             out = out*self.y_std + self.y_mean
         self.net.stream.synchronize()
         logc = 2.0*np.log(np.abs(cols["contrast"]))

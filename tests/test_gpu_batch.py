@@ -89,3 +89,46 @@ def test_batch_rejects_changed_structure(cuda):
     bad[0][key] = bad[0][key] + 1
     with pytest.raises(ValueError):
         pop.update(bad)
+
+
+def _line_sets(model, n, seed):
+    rng = np.random.default_rng(seed)
+    base = dict(workloads.population(n_sets=8, seed=seed, max_pd_n=5)[0 if model == "ellipsoid"
+                                                                        else 1][2])
+    sets = []
+    for k in range(n):
+        q = np.sort(rng.uniform(1e-3, 0.5, int(rng.integers(20, 200))))
+        pars = {key: v for key, v in base.items() if not key.startswith("theta")
+                and not key.startswith("phi")}
+        pars["theta"] = 90.0 if k == 0 else float(rng.uniform(0, 180))
+        pars["phi"] = 0.0 if k == 0 else float(rng.uniform(0, 360))
+        sets.append((q, pars))
+    return sets
+
+
+@pytest.mark.parametrize("model", ["cylinder", "ellipsoid", "core_shell_cylinder"])
+@pytest.mark.parametrize("form, rtol", [("double", RTOL_FP64), ("float32c", 1e-5)])
+def test_line_form_against_reference_2d(cuda, model, form, rtol):
+    """The line form equals the reference's 2D kernel at q vectors (q, 0)."""
+    if model == "cylinder":
+        sets = []
+        rng = np.random.default_rng(5)
+        for k in range(6):
+            q = np.sort(rng.uniform(1e-3, 0.5, int(rng.integers(20, 200))))
+            sets.append((q, dict(radius=float(rng.uniform(10, 300)),
+                                 length=float(rng.uniform(20, 3000)),
+                                 radius_pd=0.1*k/5, radius_pd_n=7,
+                                 length_pd=0.2*k/5, length_pd_n=9, sld=3.0, sld_solvent=0.0,
+                                 theta=90.0 if k < 2 else float(rng.uniform(0, 180)),
+                                 phi=0.0 if k < 2 else float(rng.uniform(0, 360)))))
+    else:
+        sets = _line_sets(model, 5, 7)
+    pop = Population(model, sets, form=form, line=True, items_per_warp=16)
+    pop.run()
+    info = load_info(model)
+    for (q, pars), raw, iq in zip(sets, pop.raw(), pop.iq()):
+        ref = reference_raw(model, info, [q, np.zeros_like(q)], pars, threads=4)
+        nq = len(q)
+        ours = np.concatenate([raw[0:2*nq:2], raw[2*nq:]])
+        worst, f2rel = compare_raw(ours, ref, 1, nq, rtol)
+        assert worst <= 1.0, (model, form, pars, worst, f2rel)

@@ -169,3 +169,15 @@ def test_abi_rejects_bad_arguments_without_gpu():
         lib.call("Iq", 10, 0, 3, 1, 1, 1, 1, 0.0, 0, 1, 1 << 20, 0x10307, None)
     with pytest.raises(RuntimeError, match="workspace"):
         lib.call("Iq", 10, 0, 3, 1, 1, 1, 1, 0.0, 0, 1, 16, 0, None)
+
+
+def test_line_form_refuses_orientation_dispersion():
+    from sasmodels_b200.batch import line_call_args
+    from sasmodels_b200.core import load_model_info
+    info = load_model_info("cylinder")
+    q = np.linspace(0.01, 0.2, 5)
+    details, values = line_call_args(info, dict(radius=20, radius_pd=0.1, radius_pd_n=5,
+                                                theta=30, phi=10), q)
+    assert details.num_eval == 5
+    with pytest.raises(ValueError, match="orientation dispersion"):
+        line_call_args(info, dict(radius=20, theta=30, theta_pd=5, theta_pd_n=3), q)

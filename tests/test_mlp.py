@@ -166,3 +166,50 @@ def test_tc_training_reduces_loss(cuda):
     last = float(loss.item())
     assert net.errors() == 0
     assert last < first/10, (first, last)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n, blocks", [(300, 0), (5000, 3), (128*300 + 17, 0)])
+def test_tc_infer_matches_forward(cuda, n, blocks):
+    """The persistent pipelined inference kernel computes the training
+    forward's outputs (same MMAs in the same order; the output dot is summed
+    in two halves), for ragged n, several tiles per CTA and one tile per CTA."""
+    from sasmodels_b200.surrogate import pad128
+    rng = np.random.default_rng(11)
+    net, W, b, w_out, b_out = _gpu_net(rng)
+    n_pad = pad128(n)
+    x, xlo, xh, _ = _inputs(rng, n, n_pad)
+    # the kernels run on net.stream: synchronise before reading or copying
+    fwd = net.forward(x, xlo, n)
+    net.stream.synchronize()
+    a = fwd.cpu().numpy()[:n].copy()
+    inf = net.infer(x, xlo, n, blocks=blocks)
+    net.stream.synchronize()
+    assert net.errors() == 0
+    c = inf.cpu().numpy()[:n]
+    np.testing.assert_allclose(c, a, rtol=1e-5, atol=1e-5*np.abs(a).max())
+    ref, _, _ = mlp_ref.forward(xh[:min(n, 2000)], [mlp_ref.bf16(w) for w in W],
+                                [np.float32(v).astype(np.float64) for v in b],
+                                np.float32(w_out).astype(np.float64), np.float32(b_out))
+    assert np.abs(c[:len(ref)] - ref).max()/np.abs(ref).max() < 2e-2
+
+
+@pytest.mark.gpu
+def test_tc_infer_tracks_training(cuda):
+    """The weight image is refreshed after training steps."""
+    import torch
+    from sasmodels_b200.surrogate import pad128
+    rng = np.random.default_rng(12)
+    net, *_ = _gpu_net(rng)
+    n = 1000
+    x, xlo, _, _ = _inputs(rng, n, pad128(n))
+    y = torch.as_tensor(rng.normal(size=pad128(n)), dtype=torch.float32, device="cuda")
+    def host(t):
+        net.stream.synchronize()
+        return t.cpu().numpy()[:n].copy()
+    before = host(net.infer(x, xlo, n))
+    net.train_step(x, xlo, y, n, 1e-2)
+    after = host(net.infer(x, xlo, n))
+    fwd = host(net.forward(x, xlo, n))
+    assert not np.array_equal(before, after)
+    np.testing.assert_allclose(after, fwd, rtol=1e-5, atol=1e-5*np.abs(fwd).max())
