@@ -32,6 +32,8 @@ from .direct_model import make_call_args
 
 SET_FIELDS = 8
 ITEM_FIELDS = 4
+#: rule length up to which one lane walks a whole quadrature (sas_batch.cuh)
+SHORT_RULE = 76
 FORMS = {"double": 0, "float32c": 1}
 LINE_FORMS = {"double": 2, "float32c": 3}
 
@@ -62,18 +64,109 @@ def rule_points(qr):
     return np.where(qr < 10, 20, np.where(qr < 100, 76, np.where(qr < 750, 500, 5000)))
 
 
+def _check_line(info, details):
+    kpars = info.parameters.kernel_parameters
+    for d in range(details.num_active):
+        p = kpars[int(details.pd_par[d])]
+        if p.type == "orientation" and details.pd_length[d] > 1:
+            raise ValueError("line form: %s has orientation dispersion" % p.name)
+
+
 def line_call_args(info, pars, q):
     """(details, values) of one line-form set: marshaled as a 2D call at
     (q, 0); orientation dispersion is refused (the line form has no jitter
     rotation)."""
     q = np.asarray(q, 'd')
     details, values, _ = make_call_args(info, pars, [q, np.zeros_like(q)])
-    kpars = info.parameters.kernel_parameters
-    for d in range(details.num_active):
-        p = kpars[int(details.pd_par[d])]
-        if p.type == "orientation" and details.pd_length[d] > 1:
-            raise ValueError("line form: %s has orientation dispersion" % p.name)
+    _check_line(info, details)
     return details, values
+
+
+def host_pack(model, info, sets, line=False, warps=8, items_per_warp=8, sms=148):
+    """
+    The flat arrays of a population (see csrc/sas_batch.cuh) built on the
+    host: per-set marshaling through pack.bulk_call_args (bitwise the
+    arrays of make_call_args), and the work items cut by the cost model.
+    Returns a dict of numpy arrays and sizes.
+    """
+    from .pack import bulk_call_args
+    qs = [np.ascontiguousarray(q, 'd').ravel() for q, _ in sets]
+    args = bulk_call_args(info, [p for _, p in sets], "2d" if line else "1d")
+    if line:
+        for d in {id(a[0]): a[0] for a in args}.values():
+            _check_line(info, d)
+    n = len(sets)
+    nq = np.array([q.size for q in qs], np.int64)
+    num_eval = np.array([a[0].num_eval for a in args], np.int64)
+    det_sizes = np.array([a[0].buffer.size for a in args], np.int64)
+    val_sizes = np.array([a[1].size for a in args], np.int64)
+    ntile = (nq + 31)//32
+
+    def offsets(sizes):
+        return np.concatenate(([0], np.cumsum(sizes)[:-1])).astype(np.int64)
+
+    desc = np.stack([nq, offsets(nq), offsets(det_sizes), offsets(val_sizes), num_eval,
+                     offsets(2*nq + 4), offsets(nq), offsets(ntile)], axis=1).astype(np.int32)
+    q_all = np.concatenate(qs) if n else np.zeros(0)
+    det_all = (np.concatenate([a[0].buffer for a in args]).astype(np.int32) if n
+               else np.zeros(0, np.int32))
+    val_all = np.concatenate([a[1] for a in args]) if n else np.zeros(0)
+    # Gauss rule points per q (one node per q for the line form)
+    pts = np.ones(q_all.size)
+    if not line and n:
+        rmax = np.repeat(np.array([_rmax(model, p, info) for _, p in sets]), nq)
+        pts = np.where(rmax > 0, rule_points(rmax*q_all), 1.0)
+    items, tile_off, tile_items = cut_items(nq, num_eval, pts, warps, items_per_warp, sms)
+    return dict(nq=[int(v) for v in nq], num_eval=[int(v) for v in num_eval],
+                pd_shape=[tuple(a[0].buffer) for a in args], val_sizes=list(val_sizes),
+                desc=desc, q=q_all, det=det_all, val=val_all, items=items,
+                tile_off=tile_off, tile_items=tile_items, n_tiles=int(ntile.sum()),
+                n_items=len(items), raw_size=int((2*nq + 4).sum()), iq_size=int(nq.sum()))
+
+
+def cut_items(nq, num_eval, pts, warps, items_per_warp, sms):
+    """Cut every (set, 32-q tile) into mesh ranges of similar cost and order
+    the items longest first.  pts: Gauss rule points of every q (all sets
+    concatenated).  Returns (items int32[n, 4] = set, q0, m0, m1;
+    tile_off int32[n_tiles + 1]; tile_items int32[n_items]) with each
+    tile's items listed in mesh order."""
+    nq = np.asarray(nq, np.int64)
+    num_eval = np.asarray(num_eval, np.int64)
+    ntile = (nq + 31)//32
+    n_tiles = int(ntile.sum())
+    warps_resident = sms*(64 // warps)*warps // 2
+    if n_tiles == 0:
+        return np.zeros((0, 4), np.int32), np.zeros(1, np.int32), np.zeros(0, np.int32)
+    tile_set = np.repeat(np.arange(len(nq)), ntile)
+    tile_first = np.arange(n_tiles) - np.repeat(np.cumsum(ntile) - ntile, ntile)
+    # q range of every tile in the concatenated q array; tiles are
+    # contiguous, so reduceat over the tile starts sums exactly one tile
+    q_start = np.repeat(np.cumsum(nq) - nq, ntile) + 32*tile_first
+    short = np.where(pts <= SHORT_RULE, pts, 0.0)
+    longc = np.where(pts > SHORT_RULE, np.ceil(pts/32.0)*_COST_NODE + _COST_REDUCE, 0.0)
+    per_point = (_COST_POINT + np.maximum.reduceat(short, q_start)*_COST_NODE
+                 + np.add.reduceat(longc, q_start))
+    n_eval = num_eval[tile_set]
+    total = float(np.sum(n_eval*per_point))
+    target = max(total/(warps_resident*items_per_warp), 1.0)
+    splits = np.minimum(n_eval, np.maximum(1, np.ceil(n_eval*per_point/target))).astype(np.int64)
+    splits[n_eval == 0] = 0
+    item_tile = np.repeat(np.arange(n_tiles), splits)
+    k = np.arange(item_tile.size) - np.repeat(np.cumsum(splits) - splits, splits)
+    s_t = splits[item_tile]
+    n_t = n_eval[item_tile]
+    m0 = (k*n_t)//s_t
+    m1 = ((k + 1)*n_t)//s_t
+    cost = (m1 - m0)*per_point[item_tile]
+    order = np.argsort(-cost, kind="stable")
+    items = np.stack([tile_set[item_tile], 32*tile_first[item_tile], m0, m1],
+                     axis=1)[order].astype(np.int32)
+    # positions of each tile's items (created in mesh order) after sorting
+    remap = np.empty(order.size, np.int64)
+    remap[order] = np.arange(order.size)
+    tile_items = remap.astype(np.int32)
+    tile_off = np.concatenate(([0], np.cumsum(splits))).astype(np.int32)
+    return items, tile_off, tile_items
 
 
 def _batch_fn(model):
@@ -122,63 +215,33 @@ class Population:
     # ---------------------------------------------------------------- pack --
     def _pack(self, sets):
         torch = self.torch
-        info = self.info
-        qs, dets, vals, desc = [], [], [], []
-        q_off = det_off = val_off = raw_off = iq_off = tile_off = 0
-        self.nq = []
-        self.num_eval = []
-        self.pd_shape = []
-        costs = []
-        for q, pars in sets:
-            q = np.ascontiguousarray(q, 'd').ravel()
-            details, values = self._marshal(pars, q)
-            nq, n_eval = q.size, details.num_eval
-            ntile = (nq + 31)//32
-            desc.append([nq, q_off, det_off, val_off, n_eval, raw_off, iq_off, tile_off])
-            qs.append(q)
-            dets.append(details.buffer.astype(np.int32))
-            vals.append(values)
-            self.nq.append(nq)
-            self.num_eval.append(n_eval)
-            self.pd_shape.append(tuple(details.buffer))
-            q_off += nq
-            det_off += details.buffer.size
-            val_off += values.size
-            raw_off += 2*nq + 4
-            iq_off += nq
-            tile_off += ntile
-            rmax = 0.0 if self.line else _rmax(self.model, pars, info)
-            pts = rule_points(q*rmax) if rmax > 0 else np.ones(nq)
-            costs.append(pts)
-        self.n_sets = len(desc)
-        self.n_tiles = tile_off
-        self._val_sizes = [v.size for v in vals]
-        items, tile_lists = self._items(desc, costs)
-        self.n_items = len(items)
-        # CSR of items per (set, tile), each in mesh order
-        off = np.zeros(self.n_tiles + 1, np.int32)
-        flat = []
-        for t in range(self.n_tiles):
-            lst = sorted(tile_lists[t], key=lambda k: items[k][2])
-            flat.extend(lst)
-            off[t + 1] = len(flat)
+        sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+        h = host_pack(self.model, self.info, sets, self.line, self.warps,
+                      self.items_per_warp, sms)
+        self.nq = h["nq"]
+        self.num_eval = h["num_eval"]
+        self.pd_shape = h["pd_shape"]
+        self._val_sizes = h["val_sizes"]
+        self.n_sets = len(self.nq)
+        self.n_tiles = h["n_tiles"]
+        self.n_items = h["n_items"]
         dev = dict(device=self.device)
         with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
-            self.d_sets = torch.as_tensor(np.array(desc, np.int32).ravel(), **dev)
-            self.d_q = torch.as_tensor(np.concatenate(qs), **dev)
-            self.d_det = torch.as_tensor(np.concatenate(dets), **dev)
-            self.h_val = torch.as_tensor(np.concatenate(vals)).pin_memory()
+            self.d_sets = torch.as_tensor(h["desc"].ravel(), **dev)
+            self.d_q = torch.as_tensor(h["q"], **dev)
+            self.d_det = torch.as_tensor(h["det"], **dev)
+            self.h_val = torch.as_tensor(h["val"]).pin_memory()
             self.d_val = self.h_val.to(self.device, non_blocking=True)
-            self.d_items = torch.as_tensor(np.array(items, np.int32).reshape(-1), **dev)
-            self.d_tile_off = torch.as_tensor(off, **dev)
-            self.d_tile_items = torch.as_tensor(np.array(flat, np.int32), **dev)
+            self.d_items = torch.as_tensor(h["items"].ravel(), **dev)
+            self.d_tile_off = torch.as_tensor(h["tile_off"], **dev)
+            self.d_tile_items = torch.as_tensor(h["tile_items"], **dev)
             f64 = dict(dtype=torch.float64, device=self.device)
             self.d_partials = torch.empty(max(64*self.n_items, 1), **f64)
             self.d_norms = torch.empty(4*self.n_sets, **f64)
-            self.d_raw = torch.empty(raw_off, **f64)
-            self.d_iq = torch.empty(iq_off, **f64)
+            self.d_raw = torch.empty(h["raw_size"], **f64)
+            self.d_iq = torch.empty(h["iq_size"], **f64)
             self.d_counter = torch.zeros(1, dtype=torch.int32, device=self.device)
-        self.desc = np.array(desc)
+        self.desc = h["desc"]
         self.stream.synchronize()
 
     def _marshal(self, pars, q):
@@ -186,41 +249,6 @@ class Population:
             details, values, _ = make_call_args(self.info, pars, [q])
             return details, values
         return line_call_args(self.info, pars, q)
-
-    def _items(self, desc, costs):
-        """Cut every (set, tile) into mesh ranges of similar cost."""
-        torch = self.torch
-        sms = torch.cuda.get_device_properties(self.device).multi_processor_count
-        warps_resident = sms*(64 // self.warps)*self.warps // 2
-        tile_cost = []
-        for s, (nq, _, _, _, n_eval, _, _, tile0) in enumerate(desc):
-            pts = costs[s]
-            for t in range((nq + 31)//32):
-                p = pts[32*t:32*t + 32]
-                short = p[p <= 76]
-                long_ = p[p > 76]
-                per_point = (_COST_POINT + (short.max() if short.size else 0)*_COST_NODE
-                             + np.sum(np.ceil(long_/32.0)*_COST_NODE + _COST_REDUCE))
-                tile_cost.append((s, t, tile0 + t, n_eval, per_point))
-        total = sum(n*c for _, _, _, n, c in tile_cost)
-        target = max(total/(warps_resident*self.items_per_warp), 1.0)
-        items, lists, cost = [], [[] for _ in range(self.n_tiles)], []
-        for s, t, tile, n_eval, per_point in tile_cost:
-            if n_eval == 0:
-                continue
-            splits = int(min(n_eval, max(1, np.ceil(n_eval*per_point/target))))
-            bounds = np.linspace(0, n_eval, splits + 1).astype(int)
-            for a, b in zip(bounds[:-1], bounds[1:]):
-                if b > a:
-                    lists[tile].append(len(items))
-                    items.append((s, 32*t, int(a), int(b)))
-                    cost.append((b - a)*per_point)
-        order = np.argsort(-np.array(cost), kind="stable") if cost else []
-        remap = np.empty(len(items), np.int64)
-        remap[order] = np.arange(len(items))
-        items = [items[k] for k in order]
-        lists = [[int(remap[k]) for k in lst] for lst in lists]
-        return items, lists
 
     # ----------------------------------------------------------------- run --
     def run(self):

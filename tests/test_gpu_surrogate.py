@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 
 def test_surrogate_gain(cuda):
     from sasmodels_b200.surrogate import train_and_evaluate
-    S, rep = train_and_evaluate(n_train_sets=3000, nq=400, epochs=4, n_holdout_sets=150,
+    S, rep = train_and_evaluate(n_train_sets=3000, nq=400, epochs=4, n_holdout_sets=600,
                                 seed=0, low_pd_frac=0.4)
     assert S.net.errors() == 0
     # a few seconds of training already predicts log I to a few percent
@@ -26,6 +26,9 @@ def test_surrogate_gain(cuda):
     op = rep["operating_points"]["0.05"]
     assert op["frac_within"] > 0.99, rep
     assert 0.0 <= op["fallback_frac"] < 1.0
+    # the calibrated gate keeps the accepted points within tolerance (the
+    # bound is statistical: 400 calibration sets at this size)
+    assert op["accepted_frac_within"] > 0.98, rep
 
 
 def test_surrogate_fallback_is_exact_where_used(cuda):
@@ -38,8 +41,10 @@ def test_surrogate_fallback_is_exact_where_used(cuda):
     sets["radius"][:] = 400.0              # outside the [10, 300] training range
     qs = [sample_q(50, rng) for _ in range(4)]
     cols = flatten(sets, qs)
-    S.edges = [np.linspace(0, 1, 3), np.linspace(-10, 10, 3)]
-    S.table = np.zeros((2, 2, 2))          # trust everything inside the domain
+    from sasmodels_b200.surrogate import MLP
+    S.gate = MLP(seed=5, stream=S.net.stream)
+    S.cal_tols = np.array([1e-3, 1.0])     # trust everything inside the domain
+    S.cal_thresh = np.array([np.inf, np.inf])
     I, back = S.iq(cols, tol=0.01)
     assert back.all()
     ref = np.concatenate(plain_unit_iq(sets, qs, form="float32c"))*np.repeat(

@@ -181,3 +181,118 @@ def test_line_form_refuses_orientation_dispersion():
     assert details.num_eval == 5
     with pytest.raises(ValueError, match="orientation dispersion"):
         line_call_args(info, dict(radius=20, theta=30, theta_pd=5, theta_pd_n=3), q)
+
+
+def test_gate_thresholds():
+    """Per-tolerance thresholds keep the accepted points' violation rate
+    at or below alpha, and grow with the tolerance."""
+    from sasmodels_b200.surrogate import gate_thresholds
+    rng = np.random.default_rng(0)
+    err = np.exp(rng.normal(-6, 1.5, 200000))
+    r = err*np.exp(rng.normal(0, 0.5, err.size))       # a noisy predictor
+    tols = np.array([1e-3, 1e-2, 5e-2])
+    th = gate_thresholds(r, err, tols, 1e-3)
+    assert np.all(np.diff(th) >= 0)
+    for tol, t in zip(tols, th):
+        acc = r <= t
+        assert acc.any()
+        assert np.mean(err[acc] > tol) <= 1e-3 + 1e-12
+    # a useless predictor accepts nothing at a tight tolerance
+    assert gate_thresholds(np.ones(100), np.ones(100), [1e-3], 1e-3)[0] == 0.0
+
+
+def test_error_envelope():
+    from sasmodels_b200.surrogate import envelope
+    err = np.array([0., 1., 0., 0., 0., 5., 0., 0.])
+    sid = np.array([0, 0, 0, 0, 1, 1, 1, 1])
+    # the maximum spreads two places each way, never across sets
+    np.testing.assert_array_equal(envelope(err, sid, 2), [1., 1., 1., 1., 5., 5., 5., 5.])
+    np.testing.assert_array_equal(envelope(err, sid, 0), err)
+
+
+@pytest.mark.parametrize("name", ["cylinder", "ellipsoid", "core_shell_cylinder", "sphere",
+                                  "core_shell_sphere"])
+@pytest.mark.parametrize("dim", ["1d", "2d"])
+def test_bulk_call_args_equal_single(name, dim):
+    """Marshaling a population in one pass gives, set by set, the same
+    details and values (bitwise) as make_call_args."""
+    from sasmodels_b200.core import load_model_info
+    from sasmodels_b200.direct_model import make_call_args
+    from sasmodels_b200.pack import bulk_call_args
+    info = load_model_info(name)
+    rng = np.random.default_rng(7)
+    vol = [p.name for p in info.parameters.kernel_parameters if p.polydisperse]
+    orient = set(p.name for p in info.parameters.kernel_parameters if p.type == "orientation")
+    pars_list = []
+    for k in range(60):
+        pars = {}
+        for p in info.parameters.kernel_parameters:
+            if p.type == "sld":
+                pars[p.name] = float(rng.uniform(-1, 7))
+            elif p.polydisperse and p.type != "orientation":
+                pars[p.name] = float(np.exp(rng.uniform(np.log(10), np.log(500))))
+        for p in vol:
+            if rng.uniform() < 0.6:
+                pars[p + "_pd"] = float(rng.uniform(0.0, 0.35)) if k % 7 else 0.0
+                pars[p + "_pd_n"] = int(rng.choice([0, 1, 5, 35]))
+                if k % 11 == 0 and p not in orient:
+                    pars[p + "_pd_type"] = "lognormal"
+        if k % 13 == 0:                 # wide enough to clip at zero
+            pars[vol[0] + "_pd"] = 0.5
+            pars[vol[0] + "_pd_n"] = 9
+        pars_list.append(pars)
+    q = [np.zeros(1)] if dim == "1d" else [np.zeros(1), np.zeros(1)]
+    bulk = bulk_call_args(info, pars_list, dim)
+    for pars, (d, v, m) in zip(pars_list, bulk):
+        d0, v0, m0 = make_call_args(info, pars, q)
+        np.testing.assert_array_equal(d.buffer, d0.buffer)
+        assert v.dtype == v0.dtype and v.shape == v0.shape
+        assert np.array_equal(v, v0), (name, pars)
+        assert m == m0
+
+
+def test_bulk_call_args_rejects_unknown():
+    from sasmodels_b200.core import load_model_info
+    from sasmodels_b200.pack import bulk_call_args
+    with pytest.raises(TypeError, match="Unused"):
+        bulk_call_args(load_model_info("sphere"), [dict(radius=1, bogus=2)])
+
+
+@pytest.mark.parametrize("line", [False, True])
+def test_host_pack_population(line):
+    """Host packing of a population: every set's arrays equal the single-call
+    marshaling, and the work items cover each (set, tile) mesh exactly once,
+    in mesh order within the tile."""
+    from sasmodels_b200.batch import host_pack
+    from sasmodels_b200.core import load_model_info
+    from sasmodels_b200.direct_model import make_call_args
+    model = "cylinder" if line else "ellipsoid"
+    info = load_model_info(model)
+    rng = np.random.default_rng(3)
+    sets = []
+    for k in range(40):
+        q = np.sort(rng.uniform(1e-3, 0.5, int(rng.integers(1, 300))))
+        if line:
+            pars = dict(radius=float(rng.uniform(10, 300)), length=float(rng.uniform(20, 3000)),
+                        radius_pd=0.1, radius_pd_n=int(rng.choice([1, 5, 35])),
+                        length_pd=0.05*(k % 3), length_pd_n=35, theta=90.0, phi=0.0)
+        else:
+            pars = dict(radius_polar=float(rng.uniform(10, 500)),
+                        radius_equatorial=float(rng.uniform(10, 500)),
+                        radius_polar_pd=0.2*(k % 2), radius_polar_pd_n=int(rng.integers(1, 20)))
+        sets.append((q, pars))
+    h = host_pack(model, info, sets, line=line, warps=8, items_per_warp=4, sms=8)
+    items, off, lst = h["items"], h["tile_off"], h["tile_items"]
+    for s, (q, pars) in enumerate(sets):
+        d, v, _ = make_call_args(info, pars, [q, 0*q] if line else [q])
+        nq_, qo, do, vo, ne, ro, io, to = h["desc"][s]
+        assert nq_ == q.size and ne == d.num_eval
+        np.testing.assert_array_equal(h["q"][qo:qo + nq_], q)
+        np.testing.assert_array_equal(h["det"][do:do + d.buffer.size], d.buffer)
+        assert np.array_equal(h["val"][vo:vo + v.size], v)
+        for t in range((q.size + 31)//32):
+            its = items[lst[off[to + t]:off[to + t + 1]]]
+            assert np.all(its[:, 0] == s) and np.all(its[:, 1] == 32*t)
+            assert its[0, 2] == 0 and its[-1, 3] == ne
+            np.testing.assert_array_equal(its[1:, 2], its[:-1, 3])
+    assert len(lst) == len(items) == len(set(lst.tolist()))
