@@ -258,11 +258,13 @@ class MLP:
 
     def features(self, radius, length, rpd, lpd, contrast, q, flag):
         """Compensated bf16 features (hi, lo) [n_pad x 16] on the device from
-        float64 arrays."""
+        float64 arrays (host arrays, or device tensors already on this
+        network's stream)."""
         torch = self.torch
         n = len(q)
         n_pad = pad128(n)
-        arrs = [torch.as_tensor(np.ascontiguousarray(a, 'd'), device=self.device)
+        arrs = [a.contiguous() if isinstance(a, torch.Tensor) else
+                torch.as_tensor(np.ascontiguousarray(a, 'd'), device=self.device)
                 for a in (radius, length, rpd, lpd, contrast, q, flag)]
         x = torch.empty((n_pad, NIN), dtype=torch.bfloat16, device=self.device)
         x_lo = torch.empty((n_pad, NIN), dtype=torch.bfloat16, device=self.device)
@@ -344,21 +346,20 @@ def plain_unit_iq(sets, qs, device=None, form="float32c"):
     from .batch import Population
     n = len(qs)
     out = [None]*n
-    idx1 = [k for k in range(n) if sets["flag"][k]]
-    if idx1:
+    pops = []
+    # both populations are packed and enqueued before either is read back,
+    # so the host packing of the second overlaps the first one's kernels
+    for flag in (1, 0):
+        idx = [k for k in range(n) if bool(sets["flag"][k]) == bool(flag)]
+        if not idx:
+            continue
         members = [(qs[k], model_pars(sets["radius"][k], sets["length"][k], sets["rpd"][k],
-                                      sets["lpd"][k], 1)) for k in idx1]
-        pop = Population("cylinder", members, form=form, device=device)
+                                      sets["lpd"][k], flag)) for k in idx]
+        pop = Population("cylinder", members, form=form, device=device, line=not flag)
         pop.run()
-        for k, iq in zip(idx1, pop.iq()):
-            out[k] = iq.copy()
-    idx0 = [k for k in range(n) if not sets["flag"][k]]
-    if idx0:
-        members = [(qs[k], model_pars(sets["radius"][k], sets["length"][k], sets["rpd"][k],
-                                      sets["lpd"][k], 0)) for k in idx0]
-        pop = Population("cylinder", members, form=form, device=device, line=True)
-        pop.run()
-        for k, iq in zip(idx0, pop.iq()):
+        pops.append((idx, pop))
+    for idx, pop in pops:
+        for k, iq in zip(idx, pop.iq()):
             out[k] = iq.copy()
     return out
 
@@ -575,15 +576,64 @@ class Surrogate:
         self.alpha = alpha
         return err
 
+    def _accept_log_threshold(self, tol):
+        """log of the gate threshold at tolerance `tol` (the largest
+        calibrated tolerance not above it); -inf when nothing is trusted."""
+        if self.gate is None or self.cal_thresh is None:
+            return -np.inf
+        k = np.searchsorted(self.cal_tols, tol, side="right") - 1
+        if k < 0 or self.cal_thresh[k] <= 0:
+            return -np.inf
+        return float(np.log(self.cal_thresh[k]))
+
+    def _device_eval(self, cols, tol):
+        """(I, accepted mask) of the network at every point, computed on the
+        device: only q, a run index and one row per run of points sharing a
+        parameter set cross to the GPU (points of a set are contiguous, as
+        flatten() lays them out); the domain check, the gate threshold and
+        exp(log I) run there too."""
+        torch = self.torch
+        dev = self.net.device
+        sid = np.asarray(cols["set"])
+        n = len(sid)
+        new = np.r_[True, sid[1:] != sid[:-1]] if n else np.zeros(0, bool)
+        starts = np.flatnonzero(new)
+        run = (np.cumsum(new) - 1).astype(np.int32)
+        keys = ("radius", "length", "rpd", "lpd", "contrast", "flag")
+        table = np.stack([np.asarray(cols[k], float)[starts] for k in keys], axis=1)
+        ok = np.abs(table[:, 4]) > 0
+        for j, key in enumerate(keys[:5]):
+            lo, hi = DOMAIN[key]
+            ok &= (table[:, j] >= lo) & (table[:, j] <= hi)
+        table = np.concatenate([table, ok[:, None].astype(float)], axis=1)
+        thr = self._accept_log_threshold(tol)
+        qlo, qhi = DOMAIN["q"]
+        with torch.cuda.stream(self.net.stream):
+            T = torch.as_tensor(table, device=dev).index_select(
+                0, torch.as_tensor(run, device=dev))
+            q = torch.as_tensor(np.ascontiguousarray(cols["q"], 'd'), device=dev)
+            x, x_lo, _ = self.net.features(T[:, 0], T[:, 1], T[:, 2], T[:, 3], T[:, 4], q,
+                                           T[:, 5])
+            logi = (self.net.infer(x, x_lo, n)[:n].double()*self.y_std + self.y_mean
+                    + 2.0*torch.log(T[:, 4].abs()))
+            accept = (T[:, 6] > 0.5) & (q >= qlo) & (q <= qhi)
+            if np.isfinite(thr):
+                g = self.gate.infer(x, x_lo, n)[:n].double()*self.g_std + self.g_mean
+                accept &= g <= thr
+            else:
+                accept &= False
+            I = torch.exp(logi).cpu().numpy()
+            acc = accept.cpu().numpy()
+        return I, acc
+
     def iq(self, cols, tol=None, device=None, form="float32c"):
         """I(q) for flat inputs: the network where its predicted error is
         within `tol` (log I), the plain kernel elsewhere (its FP32c form by
         default, within 1e-5 of FP64, far inside the tolerance).  Returns
         (I, mask of points that fell back)."""
         tol = self.TOL if tol is None else tol
-        logi, g = self._outputs(cols)
-        back = self._predicted(cols, g) > tol
-        I = np.exp(logi)
+        I, accepted = self._device_eval(cols, tol)
+        back = ~accepted
         if back.any():
             I[back] = self.plain(cols, back, device, form)
         return I, back

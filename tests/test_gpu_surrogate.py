@@ -14,8 +14,11 @@ pytestmark = pytest.mark.gpu
 
 def test_surrogate_gain(cuda):
     from sasmodels_b200.surrogate import train_and_evaluate
+    # a net trained for seconds is far from the full one: the gate is
+    # calibrated here for 1 % violations among the accepted points (the
+    # full configuration uses 0.05 %)
     S, rep = train_and_evaluate(n_train_sets=3000, nq=400, epochs=4, n_holdout_sets=600,
-                                seed=0, low_pd_frac=0.4)
+                                seed=0, low_pd_frac=0.4, alpha=0.01)
     assert S.net.errors() == 0
     # a few seconds of training already predicts log I to a few percent
     assert rep["net_median_err"] < 0.05, rep
