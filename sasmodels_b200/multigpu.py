@@ -6,10 +6,15 @@ One process per GPU (torch.distributed) for the two ways the path shards:
   locally, curves gathered back in the caller's order;
 * one large detector image: q points split into contiguous blocks, every
   rank integrating the same dispersity mesh, the blocks gathered back (the
-  four norm sums are identical on every rank, so rank 0's are kept).
+  four norm sums are identical on every rank, so rank 0's are kept);
+* one call with few q and a large mesh: the mesh split into contiguous
+  [pd_start, pd_stop) ranges (the restart contract of kernel_iq.c:392-409),
+  each rank summing its range from zero, the partial sums gathered and
+  added in rank order, so every rank holds the same, reproducible total.
 
-Neither needs a reduction on the data path -- the only collective is the
-final gather of results.  The evaluation itself is a callable, the GPU
+The first two need no reduction on the data path -- the only collective is
+the final gather of results; the third has one small exchange (nout*nq + 4
+doubles per rank).  The evaluation itself is a callable, the GPU
 engine by default, so the host logic here runs (and is tested) with the
 gloo backend on CPU as well as NCCL on GPUs.
 """
@@ -124,3 +129,59 @@ def evaluate_image(q_vectors, evaluate):
         a, b = q_blocks(nq, size)[r]
         out.append(piece[:nout*(b - a)])
     return np.concatenate(out + [pieces[0][-4:]])
+
+
+def mesh_ranges(num_eval, nranks):
+    """Contiguous [pd_start, pd_stop) mesh ranges, one per rank."""
+    b = np.linspace(0, num_eval, nranks + 1).astype(int)
+    return [(int(b[r]), int(b[r + 1])) for r in range(nranks)]
+
+
+def evaluate_mesh(num_eval, evaluate):
+    """One call's mesh split over the process group: *evaluate(pd_start,
+    pd_stop)* returns the raw sums (F^2 [and F] slots, then the four norms)
+    of that mesh range started from zero, as a numpy array or torch tensor;
+    the ranks' partial sums are all-gathered and added in rank order, which
+    gives every rank the same total whatever the reduction hardware."""
+    import torch
+    size, rank = world()
+    lo, hi = mesh_ranges(num_eval, size)[rank]
+    part = evaluate(lo, hi)
+    if size == 1:
+        return part
+    dist = _dist()
+    as_numpy = not isinstance(part, torch.Tensor)
+    t = torch.as_tensor(np.asarray(part)) if as_numpy else part.contiguous()
+    bufs = [torch.empty_like(t) for _ in range(size)]
+    dist.all_gather(bufs, t)
+    total = bufs[0].clone()
+    for b in bufs[1:]:
+        total += b
+    return total.numpy() if as_numpy else total
+
+
+def kernel_mesh_partition(kernel, call_details, values, cutoff=0.0, magnetic=False,
+                          radius_effective_mode=0):
+    """Raw result of one B200Kernel call (the layout of ``kernel.result``,
+    in the caller's q order) with its mesh split over the process group,
+    one rank per GPU; every rank returns the same summed vector."""
+    import torch
+    variant = kernel.variant(magnetic)
+    dev_d, dev_v = kernel.upload(call_details, values)
+
+    def run(lo, hi):
+        with torch.cuda.device(kernel.device), torch.cuda.stream(kernel.stream):
+            out = torch.zeros_like(kernel._result_dev)
+            if hi > lo:
+                kernel.launch(variant, dev_d, dev_v, lo, hi, cutoff, radius_effective_mode,
+                              result_dev=out)
+        kernel.stream.synchronize()
+        return out
+
+    total = evaluate_mesh(call_details.num_eval, run).cpu().numpy()
+    raw = total.copy()
+    order = kernel.q_input.order
+    if order is not None:
+        nq = kernel.q_input.nq
+        raw[order] = total[:nq]
+    return raw

@@ -43,6 +43,7 @@ def _worker(rank, size, port, queue):
     dist.init_process_group("gloo", rank=rank, world_size=size)
     try:
         from helpers import load_info, marshal, reference_raw
+        import numpy as np
         from sasmodels_b200 import multigpu, workloads
         pop = [(q, p) for name, q, p in workloads.population(n_sets=10, seed=2, max_pd_n=4)
                if name == "ellipsoid"]
@@ -52,7 +53,17 @@ def _worker(rank, size, port, queue):
         info = load_info(name)
         raw = multigpu.evaluate_image(
             qv, lambda qb: reference_raw(name, info, qb, pars))
-        queue.put((rank, [c.tolist() for c in curves], raw.tolist()))
+        # one call's mesh split over the ranks, partial sums from the
+        # reference DLL's own restart contract (pd_start > 0 accumulates)
+        from oracle import refdll
+        name1, (q1,), pars1 = workloads.sphere_1d()
+        info1 = load_info(name1)
+        d1, v1, _ = marshal(info1, pars1, [q1])
+        dll = refdll.load(name1)
+        mesh = multigpu.evaluate_mesh(
+            d1.num_eval, lambda lo, hi: dll.call("Iq", q1, d1.buffer, v1, 2, pd_start=lo,
+                                                 pd_stop=hi, result=np.zeros(2*len(q1) + 4)))
+        queue.put((rank, [c.tolist() for c in curves], raw.tolist(), mesh.tolist()))
     finally:
         dist.destroy_process_group()
 
@@ -88,8 +99,23 @@ def test_two_rank_gloo_matches_single_process():
     single = _oracle_population("ellipsoid", pop)
     name, qv, pars = workloads.cylinder_2d(n=6, radius_n=3, length_n=3, theta_n=3, phi_n=3)
     raw_single = reference_raw(name, load_info(name), qv, pars)
-    for rank, curves, raw in results:
+    name1, (q1,), pars1 = workloads.sphere_1d()
+    mesh_single = reference_raw(name1, load_info(name1), [q1], pars1)
+    meshes = []
+    for rank, curves, raw, mesh in results:
         assert len(curves) == len(single)
         for a, b in zip(curves, single):
             np.testing.assert_array_equal(np.array(a), b)
         np.testing.assert_array_equal(np.array(raw), raw_single)
+        # the two partial sums re-associate the mesh sum: equal to rounding
+        np.testing.assert_allclose(np.array(mesh), mesh_single, rtol=1e-13, atol=0)
+        meshes.append(mesh)
+    assert meshes[0] == meshes[1]        # identical on every rank
+
+
+def test_mesh_ranges_cover():
+    from sasmodels_b200.multigpu import mesh_ranges
+    for n, r in [(35, 2), (490000, 8), (1, 4), (0, 3)]:
+        rg = mesh_ranges(n, r)
+        assert rg[0][0] == 0 and rg[-1][1] == n
+        assert all(a[1] == b[0] for a, b in zip(rg[:-1], rg[1:]))
