@@ -122,6 +122,50 @@ SASB200_DECLARE_MODEL(core_shell_sphere_f32c)
 SASB200_DECLARE_MODEL(ellipsoid_f32c)
 SASB200_DECLARE_MODEL(core_shell_cylinder_f32c)
 
+/*
+ * Batched evaluation of a whole fit population of one model in one
+ * persistent launch (five models: sphere, cylinder, core_shell_sphere,
+ * ellipsoid, core_shell_cylinder).
+ *
+ * Reference interface replaced: a population is evaluated by the reference
+ * one parameter set at a time -- bumps Experiment.theory
+ * (sasmodels/bumps_model.py:250-261) -> DataMixin._calc_theory
+ * (sasmodels/direct_model.py:319-351) -> Kernel.Fq (sasmodels/kernel.py:
+ * 101-188) -> one DLL call per set (sasmodels/kerneldll.py:449-475); this
+ * one call replaces that loop, with the per-set arrays of each of those
+ * calls concatenated.
+ *
+ *   form          0 FP64 (the plugin's own Fq per q), 1 FP32-compensated,
+ *                 2 / 3 the line form (2D kernel along qx at each set's view
+ *                 angles, no orientation dispersion) in FP64 / FP32c
+ *   warps, blocks persistent grid shape (blocks 0 = occupancy-derived)
+ *   sets          int32[8*n_sets]: nq, q_off, det_off, val_off, num_eval,
+ *                 raw_off, iq_off, tile_off of each set
+ *   q_all, det_all, val_all   concatenated q vectors, CallDetails buffers and
+ *                 values vectors of the sets (each as for a single call)
+ *   items         int32[4*n_items]: set, first q, mesh start, mesh stop
+ *   tile_items_off, tile_items   CSR list of the items of every 32-q tile
+ *                 of every set, in mesh order
+ *   partials      float64[64*n_items] scratch; norms float64[4*n_sets]
+ *   raw_all       float64[sum(2 nq + 4)]: per set the raw result layout
+ *   iq_all        float64[sum nq]: per set I(q), normalised as Kernel.Iq
+ *   counter       int32 work counter (reset by the call)
+ * Same return codes as the kernel entry points.
+ */
+#define SASB200_DECLARE_BATCH(M) \
+    int32_t sasb200_##M##_batch(int32_t form, int32_t warps, int32_t blocks, \
+        int32_t n_sets, const int32_t *sets, const double *q_all, const int32_t *det_all, \
+        const double *val_all, int32_t n_items, const int32_t *items, \
+        const int32_t *tile_items_off, const int32_t *tile_items, double cutoff, \
+        int32_t radius_effective_mode, double *partials, double *norms, double *raw_all, \
+        double *iq_all, int32_t *counter, void *stream);
+
+SASB200_DECLARE_BATCH(sphere)
+SASB200_DECLARE_BATCH(cylinder)
+SASB200_DECLARE_BATCH(core_shell_sphere)
+SASB200_DECLARE_BATCH(ellipsoid)
+SASB200_DECLARE_BATCH(core_shell_cylinder)
+
 #ifdef __cplusplus
 }
 #endif

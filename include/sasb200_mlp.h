@@ -1,0 +1,86 @@
+/*
+ * sasb200_mlp.h -- C-ABI of libsasb200_mlp.so (the learned I(q) surrogate)
+ * and of libsasb200_peaks.so (the pipe-throughput probes used as roofline
+ * denominators).
+ *
+ * No counterpart in the reference: sasmodels has no learned surrogate and
+ * no throughput probes.  The network is 16 (7 used) -> 4 x 256 SiLU -> 1
+ * with BF16 operands, compensated (hi + lo) BF16 activations and FP32
+ * accumulation in tensor memory (tcgen05).  All pointers are device
+ * pointers; bf16 tensors are passed as void*.  Every function returns 0 on
+ * success, -1 for a bad argument, -3 for a CUDA launch error;
+ * sasb200_mlp_last_error() describes the last failure on the calling host
+ * thread.  Kernels with pipeline waits write a nonzero value to *err when a
+ * bounded wait runs out (the kernel then unwinds instead of hanging).
+ * n_pad is n rounded up to a multiple of 128 (one tile of rows).
+ */
+#ifndef SASB200_MLP_H
+#define SASB200_MLP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+const char *sasb200_mlp_last_error(void);
+
+/* features: the compensated BF16 pair x + x_lo [n_pad x 16] from float64
+ * per-point inputs (radius, length, radius pd, length pd, contrast, q,
+ * orientation flag); rows >= n are zero. */
+int32_t sasb200_mlp_features(int32_t n, int32_t n_pad, const double *radius,
+                             const double *length, const double *rpd, const double *lpd,
+                             const double *drho, const double *q, const double *flag,
+                             void *x, void *x_lo, void *stream);
+
+/* inference: the weights packed once by sasb200_mlp_pack into an image of
+ * sasb200_mlp_image_bytes() bytes (16-byte aligned); out[n]; persistent
+ * grid of at most `blocks` CTAs (0 = one per SM). */
+int32_t sasb200_mlp_image_bytes(void);
+int32_t sasb200_mlp_pack(const void *w0, const void *w1, const void *w2, const void *w3,
+                         void *img, void *stream);
+int32_t sasb200_mlp_infer(int32_t n, int32_t n_pad, const void *x, const void *x_lo,
+                          const void *img, const float *const *b, const float *w_out,
+                          const float *b_out, float *out, int32_t *err, int32_t blocks,
+                          void *stream);
+
+/* training: forward with saved pre-activations and activations
+ * (z_save, h_save: [4][n_pad x 256] bf16 each, or both NULL), backward
+ * through the hidden layers (wt: transposed bf16 weights), weight
+ * gradients as split-K partial GEMMs C[splits][M x nb] = A[M x K] B[nb x K]^T,
+ * row sums / dots, Huber loss gradient, Adam (also refreshing the bf16
+ * copies w and, if non-NULL, the transposed wt). */
+int32_t sasb200_mlp_forward(int32_t n, int32_t n_pad, const void *x, const void *x_lo,
+                            const void *const *w, const float *const *b, const float *w_out,
+                            const float *b_out, float *out, void *z_save, void *h_save,
+                            int32_t *err, void *stream);
+int32_t sasb200_mlp_backward(int32_t n, int32_t n_pad, const void *const *wt,
+                             const float *w_out, const float *dout, const void *z_save,
+                             void *dz_save, int32_t *err, void *stream);
+int32_t sasb200_gemm_nt(int32_t M, int32_t nb, int32_t K, int32_t lda, int32_t ldb,
+                        const void *A, const void *B, int32_t splits, float *C, int32_t *err,
+                        void *stream);
+int32_t sasb200_transpose_bf16(int32_t rows, int32_t cols, const void *src, void *dst,
+                               void *stream);
+int32_t sasb200_row_dot(int32_t rows, int32_t cols, const void *M, const float *v, float *out,
+                        void *stream);
+int32_t sasb200_loss_grad(int32_t n, int32_t n_pad, const float *out, const float *y,
+                          float delta, float *dout, float *loss, void *stream);
+int32_t sasb200_adam(int32_t size, int32_t splits, const float *grad, float *p, float *m,
+                     float *v, float lr, float b1, float b2, float eps, int32_t step, void *w,
+                     void *wt, int32_t rows, int32_t cols, void *stream);
+
+/* libsasb200_peaks.so: dependent-chain throughput probes (FP64 FMA, FP32
+ * FMA, MUFU sine) whose measured rates are the roofline peaks of the
+ * FP64 and FP32-compensated kernels. */
+int32_t sasb200_probe_fp64_fma(double *out, int32_t blocks, int32_t iters, void *stream);
+int32_t sasb200_probe_fp32_fma(float *out, int32_t blocks, int32_t iters, void *stream);
+int32_t sasb200_probe_mufu_sin(float *out, int32_t blocks, int32_t iters, void *stream);
+int32_t sasb200_probe_threads_per_block(void);
+int32_t sasb200_probe_chains(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SASB200_MLP_H */

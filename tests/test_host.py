@@ -141,6 +141,9 @@ def test_library_exports_header_symbols(name):
     for prefix in (name, name + "_f32c"):
         for suffix in _header_suffixes():
             getattr(lib, "sasb200_%s_%s" % (prefix, suffix))
+    text = open(os.path.join(ROOT, "include", "sasb200.h")).read()
+    assert "SASB200_DECLARE_BATCH(%s)" % name in text
+    getattr(lib, "sasb200_%s_batch" % name)
     meta = _abi.load_metadata(name)
     assert meta["id"] == name
 
@@ -296,3 +299,16 @@ def test_host_pack_population(line):
             assert its[0, 2] == 0 and its[-1, 3] == ne
             np.testing.assert_array_equal(its[1:, 2], its[:-1, 3])
     assert len(lst) == len(items) == len(set(lst.tolist()))
+
+
+@pytest.mark.parametrize("lib_name", ["mlp", "peaks"])
+def test_support_libraries_export_header_symbols(lib_name):
+    """libsasb200_mlp.so and libsasb200_peaks.so load without a GPU and
+    export every function include/sasb200_mlp.h declares for them."""
+    text = open(os.path.join(ROOT, "include", "sasb200_mlp.h")).read()
+    names = sorted(set(re.findall(r"\b(sasb200_\w+)\(", text)))
+    want = [n for n in names if n.startswith("sasb200_probe") == (lib_name == "peaks")]
+    assert want
+    lib = ct.CDLL(os.path.join(_abi.LIB_DIR, "libsasb200_%s.so" % lib_name))
+    for n in want:
+        getattr(lib, n)
