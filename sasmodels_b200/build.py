@@ -149,7 +149,8 @@ def build_support(force=False):
     """Libraries that do not depend on a model plugin."""
     return [build_plain("peaks.cu", "libsasb200_peaks.so", force),
             build_plain("mlp.cu", "libsasb200_mlp.so", force,
-                        extra_deps=("tc_ptx.cuh",))]
+                        extra_deps=("tc_ptx.cuh",)),
+            build_plain("resolution.cu", "libsasb200_resolution.so", force)]
 
 
 def _read(path):

@@ -1,0 +1,122 @@
+// Resolution smearing on the GPU, the step that follows the kernel in every
+// fit (sasmodels/direct_model.py:345 -> Resolution.apply).
+//
+//   pinhole_smear       1D pinhole (sasmodels/resolution.py:172-220): each
+//                       measured q_i averages the theory over the calculated
+//                       points q_calc[j] within [q_i - 2.5 s_i, q_i + 3 s_i],
+//                       weighted by the gaussian mass of each point's bin,
+//                       erf((e[j+1] - q_i)/(sqrt2 s_i)) - erf((e[j] - q_i)/(sqrt2 s_i)),
+//                       normalised by the weights' sum.  The reference builds
+//                       the dense n_calc x nq matrix and multiplies; here one
+//                       warp per q_i walks only its band (computed on the host
+//                       by binary search), forming the weights on the fly: the
+//                       work is the band, not the matrix.
+//   pinhole2d_average   2D pinhole (sasmodels/resolution2d.py:162-175): the
+//                       weighted average over the nbins oversampling points of
+//                       every q, products and sums rounded separately in bin
+//                       order, as numpy's axis-0 reduction does.
+//
+// Both read theory values the model kernel left on the device, so a fit step
+// needs no host round trip between the kernel and the smearing.
+#include <cstdint>
+#include <cstdio>
+#include <cuda_runtime.h>
+
+namespace res {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr double SQRT2 = 1.4142135623730951;     // numpy sqrt(2.0), correctly rounded
+
+__global__ void __launch_bounds__(256)
+pinhole_smear(int nq, const double *__restrict__ q, const double *__restrict__ width,
+              const int32_t *__restrict__ lo, const int32_t *__restrict__ hi,
+              const double *__restrict__ edges, const double *__restrict__ theory,
+              double *__restrict__ out)
+{
+    const int i = (int)((blockIdx.x*(size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= nq) return;                      // whole warps leave together
+    const double qi = q[i];
+    const double s = SQRT2*width[i];
+    double acc = 0.0, wsum = 0.0;
+    for (int j = lo[i] + lane; j < hi[i]; j += 32) {
+        const double w = erf((edges[j + 1] - qi)/s) - erf((edges[j] - qi)/s);
+        acc += w*theory[j];
+        wsum += w;
+    }
+    #pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        acc += __shfl_xor_sync(FULL, acc, off);
+        wsum += __shfl_xor_sync(FULL, wsum, off);
+    }
+    if (lane == 0) out[i] = acc/wsum;
+}
+
+__global__ void __launch_bounds__(256)
+pinhole2d_average(int nq, int nbins, const double *__restrict__ theory,
+                  const double *__restrict__ weights, double wsum, double *__restrict__ out)
+{
+    const int i = (int)(blockIdx.x*(size_t)blockDim.x + threadIdx.x);
+    if (i >= nq) return;
+    double num = __dmul_rn(theory[i], weights[0]);
+    for (int b = 1; b < nbins; ++b)
+        num = __dadd_rn(num, __dmul_rn(theory[(size_t)b*nq + i], weights[b]));
+    out[i] = num/wsum;
+}
+
+inline char *errbuf()
+{
+    static thread_local char buf[256] = "";
+    return buf;
+}
+
+inline int32_t status(const char *what)
+{
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        std::snprintf(errbuf(), 256, "%s: %s", what, cudaGetErrorString(e));
+        return -3;
+    }
+    return 0;
+}
+
+}  // namespace res
+
+extern "C" {
+
+const char *sasb200_resolution_last_error(void) { return res::errbuf(); }
+
+// out[nq] = smeared theory; lo/hi: band [lo_i, hi_i) of calculated points of
+// each q (0 <= lo_i <= hi_i <= n_calc); edges[n_calc + 1]; theory[n_calc].
+int32_t sasb200_pinhole_smear(int32_t nq, int32_t n_calc, const double *q, const double *width,
+                              const int32_t *lo, const int32_t *hi, const double *edges,
+                              const double *theory, double *out, void *stream)
+{
+    res::errbuf()[0] = 0;
+    if (nq < 0 || n_calc < 0 || (nq > 0 && (!q || !width || !lo || !hi || !edges || !theory
+                                            || !out)))
+        return (std::snprintf(res::errbuf(), 256, "bad arguments"), -1);
+    if (nq == 0) return 0;
+    const int threads = 256;
+    const long long warps = nq;
+    const unsigned blocks = (unsigned)((warps*32 + threads - 1)/threads);
+    res::pinhole_smear<<<blocks, threads, 0, (cudaStream_t)stream>>>(nq, q, width, lo, hi,
+                                                                      edges, theory, out);
+    return res::status("pinhole_smear");
+}
+
+// out[nq] = sum_b weights[b] theory[b*nq + i] / wsum, bins in order.
+int32_t sasb200_pinhole2d_average(int32_t nq, int32_t nbins, const double *theory,
+                                  const double *weights, double wsum, double *out, void *stream)
+{
+    res::errbuf()[0] = 0;
+    if (nq < 0 || nbins < 1 || (nq > 0 && (!theory || !weights || !out)))
+        return (std::snprintf(res::errbuf(), 256, "bad arguments"), -1);
+    if (nq == 0) return 0;
+    const int threads = 256;
+    res::pinhole2d_average<<<(nq + threads - 1)/threads, threads, 0, (cudaStream_t)stream>>>(
+        nq, nbins, theory, weights, wsum, out);
+    return res::status("pinhole2d_average");
+}
+
+}  // extern "C"
