@@ -419,6 +419,47 @@ def population_compare(n_sets, stride, dev, tune=True):
             "autotuned": tuned}
 
 
+def smear_compare(dev, reps=50):
+    """One smeared sphere 1D curve (1000 q, 5 % pinhole, 35-point
+    dispersity) through the model kernel and the GPU smearing with only the
+    smeared curve read back, against the same kernel followed by the
+    reference's dense-matrix smearing on the host (theory read back)."""
+    import torch
+    from sasmodels_b200 import load_model, workloads
+    from sasmodels_b200.resolution import Pinhole1D
+    name, (q,), pars = workloads.sphere_1d()
+    res = Pinhole1D(q, 0.05*q, device=dev)
+    W = res.weight_matrix
+    model = load_model(name, device=dev)
+    kernel = model.make_kernel([res.q_calc])
+    details, values, _ = marshal(model.info, pars, [res.q_calc])
+    dd, dv = kernel.upload(details, values)
+
+    def fused():
+        I = kernel.Iq_device(dd, dv, details.num_eval, values[0], values[1])
+        out = res.apply(I, stream=kernel.stream)
+        kernel.stream.synchronize()
+        return out.cpu().numpy()
+
+    def host():
+        I = kernel.Iq_device(dd, dv, details.num_eval, values[0], values[1])
+        kernel.stream.synchronize()
+        return np.dot(I.cpu().numpy()[None, :], W).flatten()
+
+    out = {"n_q": len(q), "n_calc": len(res.q_calc)}
+    for key, fn in (("gpu_smear_ms", fused), ("host_matrix_smear_ms", host)):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        out[key] = 1e3*(time.perf_counter() - t0)/reps
+    a, b = fused(), host()
+    out["max_rel_diff"] = float(np.max(np.abs(a - b)/np.abs(b)))
+    return out
+
+
 def extras(dev):
     """Secondary measurements of the other headline configurations."""
     from sasmodels_b200 import workloads
@@ -432,6 +473,7 @@ def extras(dev):
         out["magnetic_" + dtype] = {"evals_per_s": v, "ms_per_call": 1e3*t,
                                     "spin_channels": 6}
     out["population"] = population_compare(4096, 7, dev)
+    out["smear_pinhole1d"] = smear_compare(dev)
     return out
 
 

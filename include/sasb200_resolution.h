@@ -10,6 +10,11 @@
  *                              measured q (lo[i] <= j < hi[i]) replaces the
  *                              dense n_calc x nq matrix and the weights are
  *                              formed on the fly from the bin edges.
+ *   sasb200_slit_smear         Slit1D.apply with the matrix of
+ *                              slit_resolution (sasmodels/resolution.py:
+ *                              168-169, 223-395); q_calc is the signed,
+ *                              sorted calculation grid, n_length the steps
+ *                              across the slit width (30 in the reference).
  *   sasb200_pinhole2d_average  Pinhole2D.apply (sasmodels/resolution2d.py:
  *                              162-175): np.average over the oversampling
  *                              bins, theory laid out bin-major [nbins][nq],
@@ -32,6 +37,11 @@ const char *sasb200_resolution_last_error(void);
 int32_t sasb200_pinhole_smear(int32_t nq, int32_t n_calc, const double *q, const double *width,
                               const int32_t *lo, const int32_t *hi, const double *edges,
                               const double *theory, double *out, void *stream);
+
+int32_t sasb200_slit_smear(int32_t nq, int32_t n_calc, const double *q, const double *width,
+                           const double *length, int32_t n_length, const double *q_calc,
+                           const double *edges, const double *theory, double *out,
+                           void *stream);
 
 int32_t sasb200_pinhole2d_average(int32_t nq, int32_t nbins, const double *theory,
                                   const double *weights, double wsum, double *out,

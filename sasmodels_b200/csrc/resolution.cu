@@ -11,6 +11,10 @@
 //                       warp per q_i walks only its band (computed on the host
 //                       by binary search), forming the weights on the fly: the
 //                       work is the band, not the matrix.
+//   slit_smear          1D slit (sasmodels/resolution.py:223-395): per q_i
+//                       and per step across the slit width, the bins between
+//                       |q| and sqrt(q^2 + l^2) found by binary search, the
+//                       u-substituted bin widths formed on the fly.
 //   pinhole2d_average   2D pinhole (sasmodels/resolution2d.py:162-175): the
 //                       weighted average over the nbins oversampling points of
 //                       every q, products and sums rounded separately in bin
@@ -64,6 +68,72 @@ pinhole2d_average(int nq, int nbins, const double *__restrict__ theory,
     out[i] = num/wsum;
 }
 
+// Binary search: first index in edges[0..n) with edges[k] >= x (or > x
+// when strict), the same in every lane.
+__device__ __forceinline__ int lower_edge(const double *edges, int n, double x, bool strict)
+{
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const bool before = strict ? edges[mid] <= x : edges[mid] < x;
+        if (before) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// u(e) of the slit integral (sasmodels/resolution.py:387-395): e^2 - q^2
+// inside [|q|, sqrt(q^2 + l^2)], 0 below, (limit^2 - q^2) above.  Each
+// product and difference is rounded on its own (no contraction into an
+// FMA): sqrt(u) near the lower limit amplifies the last bit of u.
+__device__ __forceinline__ double sq_diff(double a, double b)
+{
+    return __dsub_rn(__dmul_rn(a, a), __dmul_rn(b, b));
+}
+
+__device__ __forceinline__ double slit_u(double e, double qk, double limit)
+{
+    if (e < fabs(qk)) return 0.0;
+    if (e > limit) return sq_diff(limit, qk);
+    return sq_diff(e, qk);
+}
+
+__global__ void __launch_bounds__(256)
+slit_smear(int nq, int n_calc, const double *__restrict__ q, const double *__restrict__ width,
+           const double *__restrict__ length, int n_length, const double *__restrict__ q_calc,
+           const double *__restrict__ edges, const double *__restrict__ theory,
+           double *__restrict__ out)
+{
+    const int i = (int)((blockIdx.x*(size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= nq) return;
+    const double qi = q[i], wi = width[i], li = length[i];
+    double acc = 0.0;
+    if (wi == 0.0 && li == 0.0) {
+        // perfect resolution: the theory at q_calc == q
+        for (int j = lane; j < n_calc; j += 32)
+            if (q_calc[j] == qi) acc += theory[j];
+    } else {
+        const int kmax = wi == 0.0 ? 0 : n_length;
+        for (int k = -kmax; k <= kmax; ++k) {
+            const double qk = kmax ? qi + (k*wi)/n_length : qi;
+            const double limit = sqrt(__dadd_rn(__dmul_rn(qk, qk), __dmul_rn(li, li)));
+            // bins whose u changes: from the last edge below |qk| to the
+            // first edge above the limit
+            const int a = max(lower_edge(edges, n_calc + 1, fabs(qk), false) - 1, 0);
+            const int b = min(lower_edge(edges, n_calc + 1, limit, true), n_calc);
+            for (int j = a + lane; j < b; j += 32) {
+                const double w = __dsub_rn(sqrt(slit_u(edges[j + 1], qk, limit)),
+                                           sqrt(slit_u(edges[j], qk, limit)))/li;
+                acc += w*theory[j];
+            }
+        }
+        acc /= (double)(2*kmax + 1);
+    }
+    #pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(FULL, acc, off);
+    if (lane == 0) out[i] = acc;
+}
+
 inline char *errbuf()
 {
     static thread_local char buf[256] = "";
@@ -103,6 +173,28 @@ int32_t sasb200_pinhole_smear(int32_t nq, int32_t n_calc, const double *q, const
     res::pinhole_smear<<<blocks, threads, 0, (cudaStream_t)stream>>>(nq, q, width, lo, hi,
                                                                       edges, theory, out);
     return res::status("pinhole_smear");
+}
+
+// Slit smearing: out[i] = sum_j W[i, j] theory[j] with the slit weights of
+// sasmodels/resolution.py:223-395 (length only, or width and length with
+// 2 n_length + 1 steps across the width); q_calc[n_calc] sorted, edges
+// [n_calc + 1].  A nonzero width with a zero length is refused on the host,
+// as by the reference.
+int32_t sasb200_slit_smear(int32_t nq, int32_t n_calc, const double *q, const double *width,
+                           const double *length, int32_t n_length, const double *q_calc,
+                           const double *edges, const double *theory, double *out,
+                           void *stream)
+{
+    res::errbuf()[0] = 0;
+    if (nq < 0 || n_calc < 0 || n_length < 1 || (nq > 0 && (!q || !width || !length || !q_calc
+                                                             || !edges || !theory || !out)))
+        return (std::snprintf(res::errbuf(), 256, "bad arguments"), -1);
+    if (nq == 0) return 0;
+    const int threads = 256;
+    const unsigned blocks = (unsigned)(((long long)nq*32 + threads - 1)/threads);
+    res::slit_smear<<<blocks, threads, 0, (cudaStream_t)stream>>>(
+        nq, n_calc, q, width, length, n_length, q_calc, edges, theory, out);
+    return res::status("slit_smear");
 }
 
 // out[nq] = sum_b weights[b] theory[b*nq + i] / wsum, bins in order.

@@ -1,8 +1,9 @@
 """
 Resolution smearing with the smearing itself on the GPU.
 
-Mirrors the reference's resolution classes (``sasmodels/resolution.py``,
-``sasmodels/resolution2d.py``): the same constructor arguments, the same
+Mirrors the reference's resolution classes (``sasmodels/resolution.py``
+Perfect1D, Pinhole1D, Slit1D; ``sasmodels/resolution2d.py`` Pinhole2D): the
+same constructor arguments, the same
 ``q``/``q_calc`` attributes and the same ``apply(theory)``, so a caller that
 builds ``Pinhole1D(q, dq)`` (or ``Pinhole2D(data)``), evaluates the model at
 ``q_calc`` and calls ``apply`` gets the same smeared curve.  ``apply`` takes
@@ -48,6 +49,8 @@ def _lib():
         lib.sasb200_pinhole_smear.argtypes = [I, I, P, P, P, P, P, P, P, P]
         lib.sasb200_pinhole_smear.restype = I
         lib.sasb200_pinhole2d_average.argtypes = [I, I, P, P, ct.c_double, P, P]
+        lib.sasb200_slit_smear.argtypes = [I, I, P, P, P, I, P, P, P, P, P]
+        lib.sasb200_slit_smear.restype = I
         lib.sasb200_pinhole2d_average.restype = I
         lib.sasb200_resolution_last_error.restype = ct.c_char_p
         _LIB = lib
@@ -103,6 +106,40 @@ def pinhole_extend_q(q, q_width, nsigma=PINHOLE_N_SIGMA):
     lo, hi = _nsigma(nsigma)
     q_min, q_max = np.min(q - lo*q_width), np.max(q + hi*q_width)
     return linear_extrapolation(q, q_min, q_max)
+
+
+def geometric_extrapolation(q, q_min, q_max, points_per_decade=None):
+    """Extend sorted q to [q_min, q_max] with geometric steps like the data's
+    average step (``resolution.py:485-543``)."""
+    q = np.sort(q)
+    data_min, data_max = q[0], q[-1]
+    if points_per_decade is None:
+        if data_max > data_min:
+            log_delta_q = (np.log(data_max) - np.log(data_min))/(len(q) - 1)
+        else:
+            log_delta_q = np.log(10.)/10
+    else:
+        log_delta_q = np.log(10.)/points_per_decade
+    if q_min < data_min:
+        if q_min < 0:
+            q_min = data_min*MINIMUM_ABSOLUTE_Q
+        n_low = int(np.ceil((np.log(q[0]) - np.log(q_min))/log_delta_q))
+        q_low = np.logspace(np.log10(q_min), np.log10(q[0]), n_low + 1)[:-1]
+    else:
+        q_low = []
+    if q_max > data_max:
+        n_high = int(np.ceil((np.log(q_max) - np.log(data_max))/log_delta_q))
+        q_high = np.logspace(np.log10(data_max), np.log10(q_max), n_high + 1)[1:]
+    else:
+        q_high = []
+    return np.concatenate([q_low, q, q_high])
+
+
+def slit_extend_q(q, q_length=0, q_width=0):
+    """Calculation points for slit smearing (``resolution.py:412-420``)."""
+    q_min = np.min(q - q_width)
+    q_max = np.max(np.sqrt((q + q_width)**2 + q_length**2))
+    return geometric_extrapolation(q, q_min, q_max)
 
 
 def _device(device):
@@ -207,6 +244,72 @@ class Pinhole1D:
             w /= np.sum(w, axis=0)[None, :]
             self._weight_matrix = w
         return self._weight_matrix
+
+
+class Slit1D:
+    """
+    Slit aperture smearing (``resolution.py:113-169``): *q_length* along the
+    slit, *q_width* across it (scalars or per point); *q_calc* estimated when
+    None.  A nonzero width with a zero length is refused, as by the
+    reference.
+    """
+
+    N_LENGTH = 30
+
+    def __init__(self, q, q_length=None, q_width=None, q_calc=None, device=None):
+        self.q_length, self.q_width = q_length, q_width
+        n = len(q)
+        width = (np.zeros(n) if q_width is None else
+                 np.ones(n)*q_width if np.isscalar(q_width) else np.asarray(q_width, 'd'))
+        length = (np.zeros(n) if q_length is None else
+                  np.ones(n)*q_length if np.isscalar(q_length) else np.asarray(q_length, 'd'))
+        if np.any((width != 0) & (length == 0)):
+            raise NotImplementedError("We do not yet handle the q_length=0.0 case for all "
+                                      "q_width.")
+        self.q = np.asarray(q, 'd').flatten()
+        q_calc = (slit_extend_q(q, q_length=length, q_width=width)
+                  if q_calc is None else np.sort(q_calc))
+        q_calc = q_calc[abs(q_calc) >= MINIMUM_ABSOLUTE_Q*np.min(self.q)]
+        self._signed_q_calc = q_calc
+        self._width = np.ascontiguousarray(width, 'd')
+        self._length = np.ascontiguousarray(length, 'd')
+        self.edges = bin_edges(q_calc)
+        self.q_calc = abs(q_calc)
+        self._device_arg = device
+        self._dev = None
+
+    @property
+    def device(self):
+        return _device(self._device_arg)
+
+    def apply(self, theory, stream=None):
+        """Smeared I(q) from I(q_calc); CUDA tensor in -> CUDA tensor out,
+        host array in -> host array out."""
+        import torch
+        on_device = isinstance(theory, torch.Tensor) and theory.is_cuda
+        t = (theory if on_device else
+             torch.as_tensor(np.ascontiguousarray(theory, 'd'), device=self.device))
+        t = t.to(torch.float64).contiguous()
+        if t.numel() != len(self.q_calc):
+            raise ValueError("theory has %d points, q_calc %d" % (t.numel(), len(self.q_calc)))
+        if self._dev is None:
+            d = dict(device=self.device)
+            self._dev = dict(q=torch.as_tensor(self.q, **d), w=torch.as_tensor(self._width, **d),
+                             l=torch.as_tensor(self._length, **d),
+                             qc=torch.as_tensor(np.ascontiguousarray(self._signed_q_calc), **d),
+                             e=torch.as_tensor(self.edges, **d))
+        d = self._dev
+        st = stream if stream is not None else torch.cuda.current_stream(self.device)
+        with torch.cuda.device(self.device), torch.cuda.stream(st):
+            out = torch.empty(len(self.q), dtype=torch.float64, device=self.device)
+            _check(_lib().sasb200_slit_smear(
+                len(self.q), t.numel(), d["q"].data_ptr(), d["w"].data_ptr(),
+                d["l"].data_ptr(), self.N_LENGTH, d["qc"].data_ptr(), d["e"].data_ptr(),
+                t.data_ptr(), out.data_ptr(), st.cuda_stream), "slit_smear")
+        if on_device:
+            return out
+        st.synchronize()
+        return out.cpu().numpy()
 
 
 class Pinhole2D:

@@ -1,11 +1,13 @@
 """
 Generate ``resolution.json`` from the reference package's own resolution
-classes (``sasmodels/resolution.py`` Pinhole1D, ``sasmodels/resolution2d.py``
-Pinhole2D) on seeded inputs:
+classes (``sasmodels/resolution.py`` Pinhole1D and Slit1D,
+``sasmodels/resolution2d.py`` Pinhole2D) on seeded inputs:
 
 * 1D: measured q, widths, the reference's q_calc, a smooth positive theory
   at q_calc (a polydisperse-sphere-like curve computed here in numpy) and
   the reference's smeared result;
+* slit: measured q, slit length and width, the reference's q_calc, a
+  theory at q_calc and the reference's slit-smeared result;
 * 2D: measured (qx, qy), (dqx, dqy), the reference's oversampling points
   and weights, a theory at those points and the reference's average.
 
@@ -53,6 +55,15 @@ def main():
         th = theory_1d(r.q_calc)
         cases_1d.append(dict(q=q.tolist(), dq=dq.tolist(), q_calc=r.q_calc.tolist(),
                              theory=th.tolist(), result=r.apply(th).tolist()))
+    cases_slit = []
+    for k, (nq, length, width) in enumerate([(120, 0.05, 0.0), (80, 0.1, 0.002),
+                                             (200, 0.02, 0.0005)]):
+        q = np.logspace(-3, np.log10(0.3), nq)
+        r = resolution.Slit1D(q, q_length=length, q_width=width)
+        th = theory_1d(r.q_calc)
+        cases_slit.append(dict(q=q.tolist(), q_length=length, q_width=width,
+                               q_calc=r.q_calc.tolist(), theory=th.tolist(),
+                               result=r.apply(th).tolist()))
     cases_2d = []
     for k, (n, acc, coords) in enumerate([(12, "Low", "polar"), (8, "Med", "polar"),
                                           (6, "Low", "cartesian")]):
@@ -69,7 +80,7 @@ def main():
                              weights=r.q_calc_weights.tolist(), theory=th.tolist(),
                              result=r.apply(th).tolist()))
     with open(os.path.join(HERE, "resolution.json"), "w") as fid:
-        json.dump(dict(pinhole1d=cases_1d, pinhole2d=cases_2d), fid)
+        json.dump(dict(pinhole1d=cases_1d, slit1d=cases_slit, pinhole2d=cases_2d), fid)
 
 
 if __name__ == "__main__":

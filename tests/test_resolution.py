@@ -120,3 +120,31 @@ def test_fused_model_and_smearing(cuda):
     W = resolution_ref.pinhole_matrix(res._signed_q_calc, q, 0.08*q)
     np.testing.assert_allclose(smeared.cpu().numpy(), resolution_ref.smear_1d(W, I_ref),
                                rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("k", range(len(GOLD["slit1d"])))
+def test_slit1d_host_and_oracle(k):
+    from oracle import resolution_ref
+    from sasmodels_b200.resolution import Slit1D
+    c = GOLD["slit1d"][k]
+    q = np.array(c["q"])
+    r = Slit1D(q, q_length=c["q_length"], q_width=c["q_width"])
+    np.testing.assert_array_equal(r.q_calc, c["q_calc"])
+    W = resolution_ref.slit_matrix(r._signed_q_calc, q, r._length, r._width)
+    got = resolution_ref.smear_1d(W, np.array(c["theory"]))
+    np.testing.assert_allclose(got, c["result"], rtol=1e-14, atol=0)
+
+
+def test_slit1d_refuses_width_without_length():
+    from sasmodels_b200.resolution import Slit1D
+    with pytest.raises(NotImplementedError):
+        Slit1D(np.linspace(0.01, 0.1, 10), q_length=0.0, q_width=0.01)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", range(len(GOLD["slit1d"])))
+def test_slit1d_gpu(cuda, k):
+    from sasmodels_b200.resolution import Slit1D
+    c = GOLD["slit1d"][k]
+    r = Slit1D(np.array(c["q"]), q_length=c["q_length"], q_width=c["q_width"])
+    np.testing.assert_allclose(r.apply(np.array(c["theory"])), c["result"], rtol=1e-12, atol=0)
