@@ -27,7 +27,13 @@ def list_models():
 
 
 def load_model_info(name, lib_dir=None):
-    """Our :class:`ModelInfo` from the JSON written beside the library."""
+    """Our :class:`ModelInfo` from the JSON written beside the library;
+    ``"P@S"`` names give the product info (``core.py:130-169``)."""
+    if "@" in name:
+        from .product import make_product_info
+        p_name, s_name = name.split("@", 1)
+        return make_product_info(load_model_info(p_name, lib_dir),
+                                 load_model_info(s_name, lib_dir))
     return ModelInfo(_abi.load_metadata(name, lib_dir))
 
 
@@ -43,6 +49,15 @@ def build_model(model_info, dtype=None, platform=PLATFORM, device=None):
     if platform not in (PLATFORM, None):
         raise ValueError("sasmodels_b200 only provides platform %r" % PLATFORM)
     info = model_info
+    composition = getattr(info, "composition", None)
+    if composition and composition[0] == "product":
+        from .product import B200ProductModel, make_product_info
+        p_info, s_info = composition[1]
+        P = build_model(p_info, dtype=dtype, device=device)
+        S = build_model(s_info, dtype=dtype, device=device)
+        if not isinstance(info, ModelInfo):
+            info = make_product_info(P.info, S.info)
+        return B200ProductModel(info, P, S)
     if not isinstance(info, ModelInfo):
         name = info.id
         if name not in _abi.available_models():

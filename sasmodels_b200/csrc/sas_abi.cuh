@@ -98,15 +98,16 @@ __host__ inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 template <class M, int VAR>
 struct Workspace {
     using L = Layout<M, VAR>;
-    size_t table, counts, norms, partial, total;
+    size_t table, counts, norms, points, partial, total;
     Workspace(int nq, long long chunk, int splits)
     {
         const long long nseg = (chunk + SEG - 1)/SEG;
         table = align256((size_t)nseg*SEG*L::NF*sizeof(double));
         counts = align256((size_t)nseg*sizeof(int));
         norms = align256((size_t)nseg*4*sizeof(double));
+        points = align256((size_t)nseg*SEG*4*sizeof(double));   // per-point norm terms
         partial = align256((size_t)(splits > 0 ? splits : 1)*L::NOUT*(size_t)nq*sizeof(double));
-        total = table + counts + norms + partial;
+        total = table + counts + norms + points + partial;
     }
 };
 
@@ -210,7 +211,12 @@ __host__ int32_t run(int32_t nq, int32_t pd_start, int32_t pd_stop,
     double *table = reinterpret_cast<double *>(base);
     int *counts = reinterpret_cast<int *>(base + ws.table);
     double *norms = reinterpret_cast<double *>(base + ws.table + ws.counts);
-    double *partial = reinterpret_cast<double *>(base + ws.table + ws.counts + ws.norms);
+    double *points = reinterpret_cast<double *>(base + ws.table + ws.counts + ws.norms);
+    double *partial = reinterpret_cast<double *>(base + ws.table + ws.counts + ws.norms
+                                                 + ws.points);
+    // the norms in the DLL's own order when an effective radius is asked for
+    double *seq = reff_mode != 0 ? points : nullptr;
+    const int points_stride = (int)(((chunk + SEG - 1)/SEG)*SEG);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int nout_nq = L::NOUT*nq;
 
@@ -221,7 +227,8 @@ __host__ int32_t run(int32_t nq, int32_t pd_start, int32_t pd_stop,
         int splits = t.splits < nseg ? t.splits : nseg;
         if (nseg > 0) {
             mesh_prepare<M, VAR><<<nseg, SEG, 0, st>>>(
-                (int)start, n, details, values, cutoff, reff_mode, table, counts, norms);
+                (int)start, n, details, values, cutoff, reff_mode, table, counts, norms,
+                seq, points_stride);
         }
         if (nq > 0 && nseg > 0) {
             dim3 grid((nq + t.lq - 1)/t.lq, splits);
@@ -231,7 +238,8 @@ __host__ int32_t run(int32_t nq, int32_t pd_start, int32_t pd_stop,
         if (nseg == 0) splits = 0;
         const int fblocks = (nout_nq + 255)/256 + 1;
         finalize<0><<<fblocks, 256, 0, st>>>(nout_nq, splits, partial, nseg, norms, result,
-                                          start > 0 ? 1 : 0);
+                                          start > 0 ? 1 : 0, nseg > 0 ? seq : nullptr, n,
+                                          points_stride);
         const cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess) {
             std::snprintf(error_buffer(), 256, "kernel launch: %s", cudaGetErrorString(err));

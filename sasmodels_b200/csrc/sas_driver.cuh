@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(SEG)
 mesh_prepare(int pd_start, int n_mesh, const int32_t *__restrict__ details,
              const double *__restrict__ values, double cutoff, int reff_mode,
              double *__restrict__ table, int *__restrict__ seg_count,
-             double *__restrict__ seg_norm)
+             double *__restrict__ seg_norm, double *__restrict__ points, int points_stride)
 {
     using L = Layout<M, VAR>;
     constexpr int MPD = M::MAX_PD;
@@ -299,6 +299,13 @@ mesh_prepare(int pd_start, int n_mesh, const int32_t *__restrict__ details,
     norm_red[1][t] = keep ? weight*form : 0.0;
     norm_red[2][t] = keep ? weight*shell : 0.0;
     norm_red[3][t] = keep ? weight*reff : 0.0;
+    if (points != nullptr && local < n_mesh) {
+        // per-point terms of the four norm sums, in mesh order, for the
+        // sequential accumulation in finalize (0 for skipped points adds
+        // nothing)
+        #pragma unroll
+        for (int k = 0; k < 4; ++k) points[(size_t)k*points_stride + local] = norm_red[k][t];
+    }
     __syncthreads();
     int base = 0, total = 0;
     #pragma unroll
@@ -471,11 +478,22 @@ iq_main(int nq, const double *__restrict__ q, const double *__restrict__ values,
 // Sum the mesh splits for each output slot in split order, reduce the
 // segment norms with a fixed tree in the last block, and store (or add, for
 // a call that continues a partly computed mesh) into result.
+//
+// With `points` (the per-point norm terms of this chunk, in mesh order) the
+// four norms are instead accumulated one point at a time from the stored
+// value, each add rounded on its own: the order of kernel_iq.c's
+// pd_norm/weighted_form/weighted_shell/weighted_radius loop (:720-734), so
+// the sums -- and the effective radius and volume ratio derived from them --
+// equal the DLL's bit for bit.  run() asks for this when an effective radius
+// is requested: P@S feeds these values to S(q), whose closed forms for the
+// hard-sphere family cancel to high order at small q R_eff and turn a
+// one-ulp difference in R_eff into ~1e-10 in S.
 template <int UNUSED = 0>
 __global__ void __launch_bounds__(256)
 finalize(int nout_nq, int splits, const double *__restrict__ partial,
          int nseg, const double *__restrict__ seg_norm,
-         double *__restrict__ result, int accumulate)
+         double *__restrict__ result, int accumulate,
+         const double *__restrict__ points, int n_points, int points_stride)
 {
     if (blockIdx.x + 1 < gridDim.x) {
         const int i = blockIdx.x*256 + threadIdx.x;
@@ -483,6 +501,16 @@ finalize(int nout_nq, int splits, const double *__restrict__ partial,
             double s = 0.0;
             for (int k = 0; k < splits; ++k) s += partial[(size_t)k*nout_nq + i];
             result[i] = accumulate ? result[i] + s : s;
+        }
+        return;
+    }
+    if (points != nullptr) {
+        if (threadIdx.x < 4) {
+            const int k = threadIdx.x;
+            const double *pk = points + (size_t)k*points_stride;
+            double acc = accumulate ? result[nout_nq + k] : 0.0;
+            for (int p = 0; p < n_points; ++p) acc = __dadd_rn(acc, pk[p]);
+            result[nout_nq + k] = acc;
         }
         return;
     }

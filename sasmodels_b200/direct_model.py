@@ -46,7 +46,9 @@ def make_call_args(model_info, pars, q_vectors, mono=False):
     building a kernel: the arrays a kernel call (or a batch) consumes."""
     dim = '2d' if len(q_vectors) == 2 else '1d'
     pars = dict(pars)
-    pars.pop(RADIUS_MODE_ID, None)
+    if RADIUS_MODE_ID not in model_info.parameters:
+        # a call argument of Fq, except for P@S where it is a parameter
+        pars.pop(RADIUS_MODE_ID, None)
     mesh = get_mesh(model_info, pars, dim=dim, mono=mono)
     return make_kernel_args(_CallShape(model_info, dim), mesh)
 

@@ -83,7 +83,8 @@ def bulk_call_args(info, pars_list, dim="1d"):
     groups = {}
     q_dummy = [np.zeros(1)] if dim == "1d" else [np.zeros(1), np.zeros(1)]
     for i, pars in enumerate(pars_list):
-        pars = {k: v for k, v in pars.items() if k != RADIUS_MODE_ID}
+        if RADIUS_MODE_ID not in allowed:
+            pars = {k: v for k, v in pars.items() if k != RADIUS_MODE_ID}
         extra = set(pars) - allowed
         if extra:
             raise TypeError("Unused parameters in call: %s" % ", ".join(sorted(extra)))

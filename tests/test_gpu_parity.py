@@ -219,3 +219,36 @@ def test_iq_device_matches_host(cuda):
     dev = kernel.Iq_device(dev_d, dev_v, details.num_eval, values[0], values[1])
     kernel.stream.synchronize()
     np.testing.assert_allclose(dev.cpu().numpy(), host, rtol=1e-14)
+
+
+@pytest.mark.parametrize("name, pars, reff_mode", [
+    ("sphere", dict(radius=60, radius_pd=0.1, radius_pd_n=35), 1),
+    ("core_shell_sphere", dict(radius=40, radius_pd=0.2, radius_pd_n=21, thickness=10,
+                               thickness_pd=0.1, thickness_pd_n=11), 2),
+    ("cylinder", dict(radius=20, radius_pd=0.1, radius_pd_n=15, length=300, length_pd=0.2,
+                      length_pd_n=17), 3),
+])
+def test_norms_in_dll_order(cuda, name, pars, reff_mode):
+    """With an effective radius requested, the four norm sums (and so R_eff
+    and the volume ratio P@S hands to S) equal the DLL's bit for bit, also
+    when a small workspace splits the mesh into restarted chunks."""
+    import torch
+    q = np.logspace(-3, np.log10(0.4), 50)
+    info = load_info(name)
+    ref = reference_raw(name, info, [q], pars, reff_mode=reff_mode)
+    ours, nout, nq, values = gpu_raw(name, [q], pars, reff_mode=reff_mode)
+    np.testing.assert_array_equal(ours[nout*nq:nout*nq + 4], ref[nout*nq:nout*nq + 4])
+    model = load_model(name)
+    kernel = model.make_kernel([q])
+    details, values, _ = marshal(model.info, pars, [q])
+    dd, dv = kernel.upload(details, values)
+    n = details.num_eval
+    small = model.lib.workspace_bytes("Iq", kernel.q_input.nq, 300, 0)
+    ws = torch.empty(small, dtype=torch.uint8, device=kernel.device)
+    out = torch.zeros(nout*nq + 4, dtype=torch.float64, device=kernel.device)
+    with torch.cuda.stream(kernel.stream):
+        model.lib.call("Iq", kernel.q_input.nq, 0, n, dd.data_ptr(), dv.data_ptr(),
+                       kernel.q_input.q_dev.data_ptr(), out.data_ptr(), 0.0, reff_mode,
+                       ws.data_ptr(), ws.numel(), 0, kernel.stream.cuda_stream)
+    kernel.stream.synchronize()
+    np.testing.assert_array_equal(out.cpu().numpy()[nout*nq:], ref[nout*nq:nout*nq + 4])
