@@ -301,6 +301,28 @@ class Population:
             with self.torch.cuda.stream(self.stream):
                 self.d_val.copy_(self.h_val, non_blocking=True)
 
+    # ------------------------------------------------------------ fitting --
+    def nllf(self, Iq, dIq, resolution=None):
+        """The fit objective of every set against one data set, computed on
+        the device after ``run()``/``replay()``: theory -> resolution
+        smearing (a ``sasmodels_b200.resolution.Pinhole1D`` whose q_calc is
+        every set's q) -> 0.5 sum(((theory - Iq)/dIq)^2)
+        (``bumps_model.py:263-282``).  Returns a numpy array, one value per
+        set."""
+        from .resolution import nllf_sets
+        nq = self.nq[0] if self.nq else 0
+        if any(n != nq for n in self.nq):
+            raise ValueError("nllf needs every set on the same q")
+        theory = self.d_iq.view(self.n_sets, nq)
+        if resolution is not None:
+            if len(resolution.q_calc) != nq:
+                raise ValueError("resolution q_calc has %d points, the sets %d"
+                                 % (len(resolution.q_calc), nq))
+            theory = resolution.apply_sets(theory, self.stream)
+        out = nllf_sets(theory, Iq, dIq, self.stream)
+        self.stream.synchronize()
+        return out.cpu().numpy()
+
     # ------------------------------------------------------------- results --
     def iq(self):
         self.stream.synchronize()

@@ -15,6 +15,8 @@
 //                       and per step across the slit width, the bins between
 //                       |q| and sqrt(q^2 + l^2) found by binary search, the
 //                       u-substituted bin widths formed on the fly.
+//   nllf_sets           the fit objective of every curve of a population
+//                       against one data set (bumps_model.py:263-282).
 //   pinhole2d_average   2D pinhole (sasmodels/resolution2d.py:162-175): the
 //                       weighted average over the nbins oversampling points of
 //                       every q, products and sums rounded separately in bin
@@ -31,15 +33,18 @@ namespace res {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr double SQRT2 = 1.4142135623730951;     // numpy sqrt(2.0), correctly rounded
 
+// One curve per blockIdx.y: theory + y*theory_stride -> out + y*out_stride.
 __global__ void __launch_bounds__(256)
 pinhole_smear(int nq, const double *__restrict__ q, const double *__restrict__ width,
               const int32_t *__restrict__ lo, const int32_t *__restrict__ hi,
               const double *__restrict__ edges, const double *__restrict__ theory,
-              double *__restrict__ out)
+              double *__restrict__ out, size_t theory_stride, size_t out_stride)
 {
     const int i = (int)((blockIdx.x*(size_t)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (i >= nq) return;                      // whole warps leave together
+    theory += blockIdx.y*theory_stride;
+    out += blockIdx.y*out_stride;
     const double qi = q[i];
     const double s = SQRT2*width[i];
     double acc = 0.0, wsum = 0.0;
@@ -134,6 +139,28 @@ slit_smear(int nq, int n_calc, const double *__restrict__ q, const double *__res
     if (lane == 0) out[i] = acc;
 }
 
+// Negative log-likelihood of each curve against one data set
+// (bumps_model.py:263-282): 0.5 sum_i ((theory_i - y_i)/dy_i)^2, one block
+// per curve, a fixed-order tree over its points.
+__global__ void __launch_bounds__(256)
+nllf_sets(int nq, const double *__restrict__ theory, size_t theory_stride,
+          const double *__restrict__ y, const double *__restrict__ dy, double *__restrict__ out)
+{
+    const double *th = theory + blockIdx.x*theory_stride;
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < nq; i += 256) {
+        const double r = (th[i] - y[i])/dy[i];
+        acc += r*r;
+    }
+    __shared__ double red[256];
+    red[threadIdx.x] = acc;
+    for (int s = 128; s > 0; s >>= 1) {
+        __syncthreads();
+        if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = 0.5*red[0];
+}
+
 inline char *errbuf()
 {
     static thread_local char buf[256] = "";
@@ -171,8 +198,44 @@ int32_t sasb200_pinhole_smear(int32_t nq, int32_t n_calc, const double *q, const
     const long long warps = nq;
     const unsigned blocks = (unsigned)((warps*32 + threads - 1)/threads);
     res::pinhole_smear<<<blocks, threads, 0, (cudaStream_t)stream>>>(nq, q, width, lo, hi,
-                                                                      edges, theory, out);
+                                                                      edges, theory, out, 0, 0);
     return res::status("pinhole_smear");
+}
+
+// The same smearing for n_sets curves at once (a fit population sharing one
+// data set): theory[s*theory_stride + j], out[s*out_stride + i].
+int32_t sasb200_pinhole_smear_sets(int32_t n_sets, int32_t nq, int32_t n_calc, const double *q,
+                                   const double *width, const int32_t *lo, const int32_t *hi,
+                                   const double *edges, const double *theory,
+                                   int64_t theory_stride, double *out, int64_t out_stride,
+                                   void *stream)
+{
+    res::errbuf()[0] = 0;
+    if (n_sets < 0 || n_sets > 65535 || nq < 0 || n_calc < 0 || theory_stride < n_calc
+        || out_stride < nq || (nq > 0 && n_sets > 0 && (!q || !width || !lo || !hi || !edges
+                                                          || !theory || !out)))
+        return (std::snprintf(res::errbuf(), 256, "bad arguments"), -1);
+    if (nq == 0 || n_sets == 0) return 0;
+    const int threads = 256;
+    const dim3 grid((unsigned)(((long long)nq*32 + threads - 1)/threads), (unsigned)n_sets);
+    res::pinhole_smear<<<grid, threads, 0, (cudaStream_t)stream>>>(
+        nq, q, width, lo, hi, edges, theory, out, (size_t)theory_stride, (size_t)out_stride);
+    return res::status("pinhole_smear_sets");
+}
+
+// out[s] = 0.5 sum_i ((theory[s*theory_stride + i] - y[i])/dy[i])^2.
+int32_t sasb200_nllf_sets(int32_t n_sets, int32_t nq, const double *theory,
+                          int64_t theory_stride, const double *y, const double *dy,
+                          double *out, void *stream)
+{
+    res::errbuf()[0] = 0;
+    if (n_sets < 0 || nq < 0 || theory_stride < nq
+        || (n_sets > 0 && (!theory || !y || !dy || !out)))
+        return (std::snprintf(res::errbuf(), 256, "bad arguments"), -1);
+    if (n_sets == 0) return 0;
+    res::nllf_sets<<<n_sets, 256, 0, (cudaStream_t)stream>>>(nq, theory, (size_t)theory_stride,
+                                                              y, dy, out);
+    return res::status("nllf_sets");
 }
 
 // Slit smearing: out[i] = sum_j W[i, j] theory[j] with the slit weights of

@@ -51,6 +51,11 @@ def _lib():
         lib.sasb200_pinhole2d_average.argtypes = [I, I, P, P, ct.c_double, P, P]
         lib.sasb200_slit_smear.argtypes = [I, I, P, P, P, I, P, P, P, P, P]
         lib.sasb200_slit_smear.restype = I
+        L = ct.c_int64
+        lib.sasb200_pinhole_smear_sets.argtypes = [I, I, I, P, P, P, P, P, P, L, P, L, P]
+        lib.sasb200_pinhole_smear_sets.restype = I
+        lib.sasb200_nllf_sets.argtypes = [I, I, P, L, P, P, P, P]
+        lib.sasb200_nllf_sets.restype = I
         lib.sasb200_pinhole2d_average.restype = I
         lib.sasb200_resolution_last_error.restype = ct.c_char_p
         _LIB = lib
@@ -227,6 +232,24 @@ class Pinhole1D:
             return out
         st.synchronize()
         return out.cpu().numpy()
+
+    def apply_sets(self, theory, stream):
+        """Smear many curves at once: *theory* a CUDA tensor [n_sets, n_calc]
+        (rows contiguous), result [n_sets, nq] on the device, on *stream*."""
+        import torch
+        n_sets, n_calc = theory.shape
+        if n_calc != len(self.q_calc) or theory.stride(1) != 1:
+            raise ValueError("theory must be [n_sets, %d] with contiguous rows" % len(self.q_calc))
+        d = self._upload()
+        nq = len(d["q"])
+        with torch.cuda.device(self.device), torch.cuda.stream(stream):
+            out = torch.empty((n_sets, nq), dtype=torch.float64, device=self.device)
+            _check(_lib().sasb200_pinhole_smear_sets(
+                n_sets, nq, n_calc, d["q"].data_ptr(), d["width"].data_ptr(),
+                d["lo"].data_ptr(), d["hi"].data_ptr(), d["edges"].data_ptr(),
+                theory.data_ptr(), theory.stride(0), out.data_ptr(), nq, stream.cuda_stream),
+                "pinhole_smear_sets")
+        return out
 
     @property
     def weight_matrix(self):
@@ -414,3 +437,22 @@ class Pinhole2D:
             return out
         st.synchronize()
         return out.cpu().numpy()
+
+
+def nllf_sets(theory, Iq, dIq, stream):
+    """0.5 sum(((theory - Iq)/dIq)^2) of every row of the CUDA tensor
+    *theory* [n_sets, nq] (``bumps_model.py:263-282``), on *stream*; returns
+    a CUDA tensor [n_sets]."""
+    import torch
+    n_sets, nq = theory.shape
+    dev = theory.device
+    with torch.cuda.device(dev), torch.cuda.stream(stream):
+        y = torch.as_tensor(np.ascontiguousarray(Iq, 'd'), device=dev)
+        dy = torch.as_tensor(np.ascontiguousarray(dIq, 'd'), device=dev)
+        if y.numel() != nq or dy.numel() != nq or theory.stride(1) != 1:
+            raise ValueError("data has %d points, theory %d" % (y.numel(), nq))
+        out = torch.empty(n_sets, dtype=torch.float64, device=dev)
+        _check(_lib().sasb200_nllf_sets(n_sets, nq, theory.data_ptr(), theory.stride(0),
+                                        y.data_ptr(), dy.data_ptr(), out.data_ptr(),
+                                        stream.cuda_stream), "nllf_sets")
+    return out
