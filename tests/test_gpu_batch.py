@@ -132,3 +132,22 @@ def test_line_form_against_reference_2d(cuda, model, form, rtol):
         ours = np.concatenate([raw[0:2*nq:2], raw[2*nq:]])
         worst, f2rel = compare_raw(ours, ref, 1, nq, rtol)
         assert worst <= 1.0, (model, form, pars, worst, f2rel)
+
+
+def test_batch_ragged_sets(cuda):
+    """Sets of 1, 31, 32, 33 and 70 q points and a monodisperse set (mesh of
+    one) in one population, against the DLL."""
+    rng = np.random.default_rng(8)
+    sets = []
+    for nq, pd_n in [(1, 5), (31, 1), (32, 7), (33, 0), (70, 3)]:
+        q = np.sort(rng.uniform(1e-3, 0.5, nq))
+        sets.append((q, dict(radius_polar=float(rng.uniform(20, 200)),
+                             radius_equatorial=float(rng.uniform(20, 200)),
+                             radius_polar_pd=0.1, radius_polar_pd_n=pd_n)))
+    pop = Population("ellipsoid", sets, form="double")
+    pop.run()
+    info = load_info("ellipsoid")
+    for (q, pars), raw in zip(sets, pop.raw()):
+        ref = reference_raw("ellipsoid", info, [q], pars)
+        worst, f2rel = compare_raw(raw, ref, 2, len(q), RTOL_FP64)
+        assert worst <= 1.0, (len(q), worst, f2rel)

@@ -252,3 +252,19 @@ def test_norms_in_dll_order(cuda, name, pars, reff_mode):
                        ws.data_ptr(), ws.numel(), 0, kernel.stream.cuda_stream)
     kernel.stream.synchronize()
     np.testing.assert_array_equal(out.cpu().numpy()[nout*nq:], ref[nout*nq:nout*nq + 4])
+
+
+def test_more_edge_cases(cuda):
+    """No q points at all; a cutoff above every weight (all points dropped:
+    zero norms, I = background as in the DLL); a restart that continues an
+    empty first range."""
+    from sasmodels_b200.direct_model import call_kernel
+    model = load_model("sphere")
+    kernel = model.make_kernel([np.zeros(0)])
+    assert kernel.q_input.nq == 0
+    assert len(call_kernel(kernel, dict(radius=50, radius_pd=0.1, radius_pd_n=5))) == 0
+    q = np.array([0.01, 0.1])
+    pars = dict(radius=50, radius_pd=0.1, radius_pd_n=5, background=0.25)
+    assert_parity("sphere", [q], pars, cutoff=1.0, threads=1)
+    kernel = model.make_kernel([q])
+    np.testing.assert_array_equal(call_kernel(kernel, pars, cutoff=1.0), [0.25, 0.25])
