@@ -460,6 +460,18 @@ def smear_compare(dev, reps=50):
     return out
 
 
+def f32c_error(name, qv, pars, dev):
+    """Max relative difference of the FP32c I(q) from the FP64 I(q)."""
+    from sasmodels_b200 import load_model
+    from sasmodels_b200.direct_model import call_kernel
+    out = []
+    for dtype in ("double", "float32c"):
+        kernel = load_model(name, dtype=dtype, device=dev).make_kernel(qv)
+        out.append(call_kernel(kernel, dict(pars)))
+        kernel.release()
+    return float(np.max(np.abs(out[1] - out[0])/np.abs(out[0])))
+
+
 def extras(dev):
     """Secondary measurements of the other headline configurations."""
     from sasmodels_b200 import workloads
@@ -467,6 +479,10 @@ def extras(dev):
     name, qv, pars = workloads.sphere_1d()
     v, t = single_config(name, qv, pars, "double", 200, dev)
     out["sphere1d_f64"] = {"evals_per_s": v, "ms_per_call": 1e3*t}
+    name, qv, pars = workloads.cylinder_2d()
+    v, t = single_config(name, qv, pars, "float32c", 3, dev)
+    out["cylinder2d_float32c"] = {"evals_per_s": v, "ms_per_call": 1e3*t,
+                                  "max_rel_err_vs_f64": f32c_error(name, qv, pars, dev)}
     name, qv, pars = workloads.core_shell_sphere_magnetic()
     for dtype in ("double", "float32c"):
         v, t = single_config(name, qv, pars, dtype, 20, dev)
@@ -547,7 +563,7 @@ def main(argv=None):
     ap.add_argument("--surrogate-holdout", type=int, default=1500)
     ap.add_argument("--surrogate-sets", type=int, default=50000,
                     help="training parameter sets (x 1000 q each)")
-    ap.add_argument("--surrogate-epochs", type=int, default=16)
+    ap.add_argument("--surrogate-epochs", type=int, default=24)
     ap.add_argument("--grid", type=int, default=256,
                     help="q grid edge for cylinder2d (smaller for profiling)")
     ap.add_argument("--no-e2e", action="store_true")
