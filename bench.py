@@ -501,7 +501,7 @@ FLOPS_PER_EVAL = {"cylinder2d": 160.8}
 #: dram read+write bytes of the dominant kernel per launch (ncu): the mesh
 #: table is read once from DRAM and then served from L2; it does not grow
 #: with the number of q points (profiles/iq_main_cylinder2d.md)
-TRAFFIC_PER_STEP = {"cylinder2d": 39.36e6}
+TRAFFIC_PER_STEP = {"cylinder2d": 40.83e6}
 
 
 def run_population(args, world, rank, local):
