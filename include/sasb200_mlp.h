@@ -33,16 +33,27 @@ int32_t sasb200_mlp_features(int32_t n, int32_t n_pad, const double *radius,
                              const double *drho, const double *q, const double *flag,
                              void *x, void *x_lo, void *stream);
 
-/* inference: the weights packed once by sasb200_mlp_pack into an image of
- * sasb200_mlp_image_bytes() bytes (16-byte aligned); out[n]; persistent
- * grid of at most `blocks` CTAs (0 = one per SM). */
+/* pipelined forward: the weights packed once by sasb200_mlp_pack into an
+ * image of sasb200_mlp_image_bytes() bytes (16-byte aligned); out[n], and
+ * for training the z/h planes [4][n_pad x 256] bf16 (both NULL for
+ * inference); persistent grid of at most `blocks` CTAs (0 = one per SM). */
 int32_t sasb200_mlp_image_bytes(void);
 int32_t sasb200_mlp_pack(const void *w0, const void *w1, const void *w2, const void *w3,
                          void *img, void *stream);
 int32_t sasb200_mlp_infer(int32_t n, int32_t n_pad, const void *x, const void *x_lo,
                           const void *img, const float *const *b, const float *w_out,
-                          const float *b_out, float *out, int32_t *err, int32_t blocks,
-                          void *stream);
+                          const float *b_out, float *out, void *z_save, void *h_save,
+                          int32_t *err, int32_t blocks, void *stream);
+
+/* pipelined backward (training): W3^T, W2^T, W1^T packed once per weight
+ * update by sasb200_mlp_pack_t into sasb200_mlp_image_t_bytes() bytes; dZ
+ * planes [4][n_pad x 256] bf16 from dout and the saved pre-activations. */
+int32_t sasb200_mlp_image_t_bytes(void);
+int32_t sasb200_mlp_pack_t(const void *wt1, const void *wt2, const void *wt3, void *img_t,
+                           void *stream);
+int32_t sasb200_mlp_backward_p(int32_t n, int32_t n_pad, const void *img_t, const float *w_out,
+                               const float *dout, const void *z_save, void *dz_save,
+                               int32_t *err, int32_t blocks, void *stream);
 
 /* training: forward with saved pre-activations and activations
  * (z_save, h_save: [4][n_pad x 256] bf16 each, or both NULL), backward

@@ -582,6 +582,8 @@ struct InferParams {
     const float *b[4];
     const float *w_out;
     const float *b_out;
+    __nv_bfloat16 *z_save;        // optional [4][n_pad x 256] pre-activations (training)
+    __nv_bfloat16 *h_save;        // optional [4][n_pad x 256] activations (training)
 };
 
 // W_l [out][in] bf16 -> the chunk image: W0 as one 256 x 16 canonical tile,
@@ -605,6 +607,25 @@ __global__ void mlp_pack(const __nv_bfloat16 *__restrict__ w0, const __nv_bfloat
         const __nv_bfloat16 *w = l == 0 ? w1 : (l == 1 ? w2 : w3);
         const int c = k/KCI;
         uint8_t *dst = img + W0_BYTES + (size_t)(l*CHUNKS_PER_LAYER + c)*CHUNK_BYTES
+                     + tc::kmajor_offset<HID>(r, k - c*KCI);
+        *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(w + r*HID + k);
+    }
+}
+
+// The 24 chunks of three 256 x 256 matrices without W0 (layers a, b, c in
+// consumption order): the transposed weights W3^T, W2^T, W1^T that the
+// pipelined backward streams.
+__global__ void mlp_pack_layers(const __nv_bfloat16 *__restrict__ wa,
+                                const __nv_bfloat16 *__restrict__ wb,
+                                const __nv_bfloat16 *__restrict__ wc, uint8_t *__restrict__ img)
+{
+    constexpr int GL = HID*(HID/8);
+    for (int j = blockIdx.x*blockDim.x + threadIdx.x; j < 3*GL; j += gridDim.x*blockDim.x) {
+        const int l = j/GL, rem = j % GL;
+        const int r = rem/(HID/8), k = 8*(rem % (HID/8));
+        const __nv_bfloat16 *w = l == 0 ? wa : (l == 1 ? wb : wc);
+        const int c = k/KCI;
+        uint8_t *dst = img + (size_t)(l*CHUNKS_PER_LAYER + c)*CHUNK_BYTES
                      + tc::kmajor_offset<HID>(r, k - c*KCI);
         *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(w + r*HID + k);
     }
@@ -679,6 +700,7 @@ mlp_infer(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
         const int quad = warp & 3, half = warp >> 2;
         const int row = 32*quad + lane;                 // TMEM lane = tile row
         const uint32_t lane_base = (uint32_t)(32*quad) << 16;
+        const size_t plane = (size_t)n_tiles*TM*HID;
         constexpr uint32_t idesc = tc::idesc_bf16(TM, HID);
         if (t == 0) ok = tc::mbar_wait(&w0_bar, 0u);
         ok = tc::bar_and(1, INF_CONSUMERS, ok);
@@ -739,9 +761,17 @@ mlp_infer(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
                     uint32_t r16[16];
                     tc::tmem_ld16(tmem + lane_base + (uint32_t)c0, r16);
                     tc::tmem_wait_ld();
-                    float h[16];
+                    float z[16], h[16];
                     #pragma unroll
-                    for (int j = 0; j < 16; ++j) h[j] = silu(__uint_as_float(r16[j]) + bias[c0 + j]);
+                    for (int j = 0; j < 16; ++j) {
+                        z[j] = __uint_as_float(r16[j]) + bias[c0 + j];
+                        h[j] = silu(z[j]);
+                    }
+                    if (prm.z_save != nullptr) {
+                        const size_t at = (size_t)l*plane + (size_t)(row0 + row)*HID + c0;
+                        save16(prm.z_save + at, z);
+                        save16(prm.h_save + at, h);
+                    }
                     if (l == 3) {
                         #pragma unroll
                         for (int j = 0; j < 16; ++j) dot = fmaf(h[j], prm.w_out[c0 + j], dot);
@@ -753,6 +783,153 @@ mlp_infer(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
                     if (half == 1) dot_half[row] = dot;
                     tc::bar_sync(2, INF_CONSUMERS);
                     if (half == 0 && row0 + row < n) out[row0 + row] = dot + dot_half[row] + *prm.b_out;
+                }
+                tc::fence_async_smem();
+                tc::fence_before_sync();
+                ok = tc::bar_and(1, INF_CONSUMERS, ok);
+                tc::fence_after_sync();
+                if (!ok) break;
+            }
+        }
+        if (!ok && t == 0) atomicExch(err, 1);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, HID);
+}
+
+// ---------------------------------------------------------------- backward --
+// mlp_backward_p: the backward pass through the three 256 x 256 layers as a
+// persistent, pipelined kernel with the structure of mlp_infer: a producer
+// warp streams the 24 chunks of W3^T, W2^T, W1^T (packed by
+// mlp_pack_layers) through the 4-stage ring, one consumer thread issues the
+// MMAs (A = dZ_l in shared memory, B = W_l^T), eight consumer warps run the
+// epilogues dZ_{l-1} = (dZ_l W_l) * silu'(z_{l-1}), reading z from the saved
+// plane and writing dZ to its plane and, for the next layer, to shared
+// memory.  The arithmetic is that of mlp_backward.
+constexpr int BWDP_SMEM = ACT_BYTES + STAGES*CHUNK_BYTES;
+constexpr int WT_IMG_BYTES = CHUNKS_PER_TILE*CHUNK_BYTES;
+
+__global__ void __launch_bounds__(INF_THREADS, 1)
+mlp_backward_p(int n, int n_tiles, const uint8_t *__restrict__ img_t,
+               const float *__restrict__ w_out, const float *__restrict__ dout,
+               const __nv_bfloat16 *__restrict__ z_save, __nv_bfloat16 *__restrict__ dz_save,
+               int *__restrict__ err)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *act = smem;
+    uint8_t *ring = smem + ACT_BYTES;
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], acc_bar;
+    __shared__ uint32_t tmem_slot;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int my_tiles = blockIdx.x < n_tiles ? (n_tiles - 1 - blockIdx.x)/gridDim.x + 1 : 0;
+
+    if (warp == 0) {
+        tc::tmem_alloc(&tmem_slot, HID);
+        tc::tmem_relinquish();
+    }
+    if (t == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::mbar_init(&acc_bar, 1);
+        tc::mbar_fence_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == INF_CONSUMERS/32) {
+        if (lane == 0) {
+            bool ok = true;
+            const int total = my_tiles*CHUNKS_PER_TILE;
+            int i = 0;
+            for (; i < total; ++i) {
+                const int s = i % STAGES, use = i/STAGES;
+                if (use > 0 && !tc::mbar_wait(&empty[s], (uint32_t)((use - 1) & 1))) {
+                    ok = false;
+                    break;
+                }
+                tc::mbar_arrive_expect_tx(&full[s], CHUNK_BYTES);
+                tc::bulk_load(ring + s*CHUNK_BYTES,
+                              img_t + (size_t)(i % CHUNKS_PER_TILE)*CHUNK_BYTES,
+                              CHUNK_BYTES, &full[s]);
+            }
+            for (int j = (i > STAGES ? i - STAGES : 0); j < i; ++j)
+                ok = tc::mbar_wait(&full[j % STAGES], (uint32_t)((j/STAGES) & 1)) && ok;
+            if (!ok) atomicExch(err, 2);
+        }
+    } else {
+        bool ok = true;
+        uint32_t acc_phase = 0;
+        int chunk = 0;                                  // used by t == 0 only
+        const int quad = warp & 3, half = warp >> 2;
+        const int row = 32*quad + lane;
+        const uint32_t lane_base = (uint32_t)(32*quad) << 16;
+        const size_t plane = (size_t)n_tiles*TM*HID;
+        constexpr uint32_t idesc = tc::idesc_bf16(TM, HID);
+        for (int k = 0; k < my_tiles && ok; ++k) {
+            const int row0 = (blockIdx.x + k*gridDim.x)*TM;
+            const size_t grow = (size_t)(row0 + row);
+            {
+                // dZ3 = dout * w_out * silu'(z3)
+                const float d = row0 + row < n ? dout[row0 + row] : 0.0f;
+                #pragma unroll 1
+                for (int c0 = 128*half; c0 < 128*half + 128; c0 += 16) {
+                    float z[16], g[16];
+                    load16(z_save + 3*plane + grow*HID + c0, z);
+                    #pragma unroll
+                    for (int j = 0; j < 16; ++j) g[j] = d*w_out[c0 + j]*dsilu(z[j]);
+                    store16(act, row, c0, g);
+                    save16(dz_save + 3*plane + grow*HID + c0, g);
+                }
+            }
+            tc::fence_async_smem();
+            tc::fence_before_sync();
+            ok = tc::bar_and(1, INF_CONSUMERS, ok);
+            tc::fence_after_sync();
+            if (!ok) break;
+            for (int l = 3; l >= 1; --l) {
+                if (t == 0) {
+                    const uint32_t a_addr = tc::smem_u32(act);
+                    for (int c = 0; c < CHUNKS_PER_LAYER; ++c, ++chunk) {
+                        const int s = chunk % STAGES;
+                        if (!tc::mbar_wait(&full[s], (uint32_t)((chunk/STAGES) & 1))) {
+                            ok = false;
+                            break;
+                        }
+                        tc::fence_after_sync();
+                        const uint32_t b_addr = tc::smem_u32(ring + s*CHUNK_BYTES);
+                        #pragma unroll
+                        for (int st = 0; st < KCI/16; ++st) {
+                            tc::mma_bf16(tmem, tc::kmajor_desc<TM>(a_addr, c*(KCI/16) + st),
+                                         tc::kmajor_desc<HID>(b_addr, st), idesc,
+                                         (c > 0 || st > 0) ? 1u : 0u);
+                        }
+                        tc::mma_commit(&empty[s]);
+                    }
+                    tc::mma_commit(&acc_bar);
+                }
+                const bool done = tc::mbar_wait(&acc_bar, acc_phase);
+                acc_phase ^= 1u;
+                tc::fence_after_sync();
+                ok = tc::bar_and(1, INF_CONSUMERS, ok && done);
+                if (!ok) break;
+                const __nv_bfloat16 *zrow = z_save + (l - 1)*plane + grow*HID;
+                __nv_bfloat16 *drow = dz_save + (l - 1)*plane + grow*HID;
+                #pragma unroll 1
+                for (int c0 = 128*half; c0 < 128*half + 128; c0 += 16) {
+                    uint32_t r16[16];
+                    tc::tmem_ld16(tmem + lane_base + (uint32_t)c0, r16);
+                    tc::tmem_wait_ld();
+                    float z[16], g[16];
+                    load16(zrow + c0, z);
+                    #pragma unroll
+                    for (int j = 0; j < 16; ++j) g[j] = __uint_as_float(r16[j])*dsilu(z[j]);
+                    if (l > 1) store16(act, row, c0, g);
+                    save16(drow + c0, g);
                 }
                 tc::fence_async_smem();
                 tc::fence_before_sync();
@@ -793,13 +970,60 @@ int32_t sasb200_mlp_pack(const void *w0, const void *w1, const void *w2, const v
 
 int32_t sasb200_mlp_image_bytes(void) { return IMG_BYTES; }
 
-// Inference: out[n] for x, x_lo [n_pad x 16] (n_pad a multiple of 128) with
-// the packed weights; persistent grid of at most `blocks` CTAs (0 = one per
+// Pack W3^T, W2^T, W1^T (bf16 [in][out]) into the chunk image the pipelined
+// backward streams (sasb200_mlp_image_t_bytes() = 24 x 16 KB).
+int32_t sasb200_mlp_pack_t(const void *wt1, const void *wt2, const void *wt3, void *img_t,
+                           void *stream)
+{
+    errbuf()[0] = 0;
+    if (!wt1 || !wt2 || !wt3 || !img_t)
+        return (std::snprintf(errbuf(), 256, "bad arguments"), -1);
+    mlp_pack_layers<<<96, 256, 0, (cudaStream_t)stream>>>(
+        static_cast<const __nv_bfloat16 *>(wt3), static_cast<const __nv_bfloat16 *>(wt2),
+        static_cast<const __nv_bfloat16 *>(wt1), static_cast<uint8_t *>(img_t));
+    return status("mlp_pack_t");
+}
+
+int32_t sasb200_mlp_image_t_bytes(void) { return WT_IMG_BYTES; }
+
+// Backward through the hidden layers, pipelined: dZ planes [4][n_pad x 256]
+// from dout[n] and the saved pre-activations; same results as
+// sasb200_mlp_backward.
+int32_t sasb200_mlp_backward_p(int32_t n, int32_t n_pad, const void *img_t, const float *w_out,
+                               const float *dout, const void *z_save, void *dz_save,
+                               int32_t *err, int32_t blocks, void *stream)
+{
+    errbuf()[0] = 0;
+    if (n < 0 || n_pad % TM || n > n_pad || !img_t || !w_out || !dout || !z_save || !dz_save
+        || !err || blocks < 0)
+        return (std::snprintf(errbuf(), 256, "bad arguments"), -1);
+    if (reinterpret_cast<uintptr_t>(img_t) % 16)
+        return (std::snprintf(errbuf(), 256, "weight image must be 16-byte aligned"), -1);
+    if (n_pad == 0) return 0;
+    const int n_tiles = n_pad/TM;
+    if (blocks == 0) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        blocks = sms > 0 ? sms : 1;
+    }
+    if (blocks > n_tiles) blocks = n_tiles;
+    cudaFuncSetAttribute(mlp_backward_p, cudaFuncAttributeMaxDynamicSharedMemorySize, BWDP_SMEM);
+    mlp_backward_p<<<blocks, INF_THREADS, BWDP_SMEM, (cudaStream_t)stream>>>(
+        n, n_tiles, static_cast<const uint8_t *>(img_t), w_out, dout,
+        static_cast<const __nv_bfloat16 *>(z_save), static_cast<__nv_bfloat16 *>(dz_save), err);
+    return status("mlp_backward_p");
+}
+
+// Forward pass: out[n] for x, x_lo [n_pad x 16] (n_pad a multiple of 128)
+// with the packed weights, and, when z_save/h_save are given, the
+// pre-activations and activations of all four layers ([4][n_pad x 256] bf16
+// each) for training; persistent grid of at most `blocks` CTAs (0 = one per
 // SM).  err receives 1 or 2 if a pipeline wait ran out.
 int32_t sasb200_mlp_infer(int32_t n, int32_t n_pad, const void *x, const void *x_lo,
                           const void *img, const float *const *b, const float *w_out,
-                          const float *b_out, float *out, int32_t *err, int32_t blocks,
-                          void *stream)
+                          const float *b_out, float *out, void *z_save, void *h_save,
+                          int32_t *err, int32_t blocks, void *stream)
 {
     errbuf()[0] = 0;
     if (n < 0 || n_pad % TM || n > n_pad || !x || !x_lo || !img || !b || !w_out || !b_out
@@ -813,6 +1037,10 @@ int32_t sasb200_mlp_infer(int32_t n, int32_t n_pad, const void *x, const void *x
     for (int l = 0; l < 4; ++l) prm.b[l] = b[l];
     prm.w_out = w_out;
     prm.b_out = b_out;
+    if ((z_save == nullptr) != (h_save == nullptr))
+        return (std::snprintf(errbuf(), 256, "z_save and h_save go together"), -1);
+    prm.z_save = static_cast<__nv_bfloat16 *>(z_save);
+    prm.h_save = static_cast<__nv_bfloat16 *>(h_save);
     const int n_tiles = n_pad/TM;
     if (blocks == 0) {
         int dev = 0, sms = 0;

@@ -58,11 +58,14 @@ def _lib():
     lib.sasb200_adam.argtypes = [I, I, P, P, P, P, F, F, F, F, I, P, P, I, I, P]
     lib.sasb200_mlp_features.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P]
     lib.sasb200_mlp_pack.argtypes = [P, P, P, P, P, P]
-    lib.sasb200_mlp_infer.argtypes = [I, I, P, P, P, P, P, P, P, P, I, P]
+    lib.sasb200_mlp_infer.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P, I, P]
+    lib.sasb200_mlp_pack_t.argtypes = [P, P, P, P, P]
+    lib.sasb200_mlp_backward_p.argtypes = [I, I, P, P, P, P, P, P, I, P]
     for name in ("sasb200_mlp_forward", "sasb200_mlp_backward", "sasb200_gemm_nt",
                  "sasb200_transpose_bf16", "sasb200_row_dot", "sasb200_loss_grad",
                  "sasb200_adam", "sasb200_mlp_features", "sasb200_mlp_pack",
-                 "sasb200_mlp_infer", "sasb200_mlp_image_bytes"):
+                 "sasb200_mlp_infer", "sasb200_mlp_image_bytes", "sasb200_mlp_pack_t",
+                 "sasb200_mlp_image_t_bytes", "sasb200_mlp_backward_p"):
         getattr(lib, name).restype = I
     lib.sasb200_mlp_last_error.restype = ct.c_char_p
     return lib
@@ -106,6 +109,8 @@ class MLP:
         self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.img = torch.empty(self.lib.sasb200_mlp_image_bytes(), dtype=torch.uint8,
                                device=self.device)
+        self.img_t = torch.empty(self.lib.sasb200_mlp_image_t_bytes(), dtype=torch.uint8,
+                                 device=self.device)
         self._packed = None
         self._infer_out = None
         self._sync_bf16()
@@ -159,6 +164,9 @@ class MLP:
         self._check(self.lib.sasb200_mlp_pack(*[w.data_ptr() for w in self.Wb],
                                               self.img.data_ptr(), self.stream.cuda_stream),
                     "mlp_pack")
+        self._check(self.lib.sasb200_mlp_pack_t(*[w.data_ptr() for w in self.WTb[1:]],
+                                                self.img_t.data_ptr(), self.stream.cuda_stream),
+                    "mlp_pack_t")
         self._packed = key
 
     def infer(self, x, x_lo, n, blocks=0):
@@ -171,7 +179,7 @@ class MLP:
         self._pack()
         self._check(self.lib.sasb200_mlp_infer(
             n, n_pad, x.data_ptr(), x_lo.data_ptr(), self.img.data_ptr(), self._ptrs(self.b),
-            self.w_out.data_ptr(), self.b_out.data_ptr(), self._infer_out.data_ptr(),
+            self.w_out.data_ptr(), self.b_out.data_ptr(), self._infer_out.data_ptr(), None, None,
             self.err.data_ptr(), int(blocks), self.stream.cuda_stream), "mlp_infer")
         return self._infer_out[:n_pad]
 
@@ -198,17 +206,21 @@ class MLP:
         self._scratch(n_pad)
         st = self.stream.cuda_stream
         lib = self.lib
-        self._check(lib.sasb200_mlp_forward(
-            n, n_pad, x.data_ptr(), x_lo.data_ptr(), self._ptrs(self.Wb), self._ptrs(self.b),
+        # forward with the z/h planes and backward through the pipelined
+        # persistent kernels (weights streamed from the packed images)
+        self._pack()
+        self._check(lib.sasb200_mlp_infer(
+            n, n_pad, x.data_ptr(), x_lo.data_ptr(), self.img.data_ptr(), self._ptrs(self.b),
             self.w_out.data_ptr(), self.b_out.data_ptr(), self.out.data_ptr(),
-            self.z_save.data_ptr(), self.h_save.data_ptr(), self.err.data_ptr(), st), "forward")
+            self.z_save.data_ptr(), self.h_save.data_ptr(), self.err.data_ptr(), 0, st),
+            "forward")
         self._check(lib.sasb200_loss_grad(n, n_pad, self.out.data_ptr(), y.data_ptr(),
                                           float(self.huber), self.dout.data_ptr(),
                                           self.sq.data_ptr(), st), "loss")
-        self._check(lib.sasb200_mlp_backward(n, n_pad, self._ptrs(self.WTb), self.w_out.data_ptr(),
-                                             self.dout.data_ptr(), self.z_save.data_ptr(),
-                                             self.dz_save.data_ptr(), self.err.data_ptr(), st),
-                    "backward")
+        self._check(lib.sasb200_mlp_backward_p(n, n_pad, self.img_t.data_ptr(),
+                                               self.w_out.data_ptr(), self.dout.data_ptr(),
+                                               self.z_save.data_ptr(), self.dz_save.data_ptr(),
+                                               self.err.data_ptr(), 0, st), "backward")
         plane = n_pad*HID
         for l in range(4):
             nb = NIN if l == 0 else HID

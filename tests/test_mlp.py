@@ -213,3 +213,45 @@ def test_tc_infer_tracks_training(cuda):
     fwd = host(net.forward(x, xlo, n))
     assert not np.array_equal(before, after)
     np.testing.assert_allclose(after, fwd, rtol=1e-5, atol=1e-5*np.abs(fwd).max())
+
+
+@pytest.mark.gpu
+def test_tc_pipelined_training_kernels_match(cuda):
+    """The pipelined forward (with z/h planes) and backward give the planes
+    of the one-CTA-per-tile training kernels bit for bit (same MMAs in the
+    same order, same epilogue arithmetic)."""
+    import ctypes as ct
+    import torch
+    from sasmodels_b200.surrogate import HID, pad128
+    rng = np.random.default_rng(13)
+    net, *_ = _gpu_net(rng)
+    n = 3000
+    n_pad = pad128(n)
+    x, xlo, _, _ = _inputs(rng, n, n_pad)
+    net._scratch(n_pad)
+    lib, st = net.lib, net.stream.cuda_stream
+    bf = dict(dtype=torch.bfloat16, device="cuda")
+    z1, h1, z2, h2 = [torch.zeros(4*n_pad*HID, **bf) for _ in range(4)]
+    o1 = torch.zeros(n_pad, dtype=torch.float32, device="cuda")
+    o2 = torch.zeros_like(o1)
+    net._check(lib.sasb200_mlp_forward(n, n_pad, x.data_ptr(), xlo.data_ptr(), net._ptrs(net.Wb),
+                                       net._ptrs(net.b), net.w_out.data_ptr(),
+                                       net.b_out.data_ptr(), o1.data_ptr(), z1.data_ptr(),
+                                       h1.data_ptr(), net.err.data_ptr(), st), "forward")
+    net._pack()
+    net._check(lib.sasb200_mlp_infer(n, n_pad, x.data_ptr(), xlo.data_ptr(), net.img.data_ptr(),
+                                     net._ptrs(net.b), net.w_out.data_ptr(),
+                                     net.b_out.data_ptr(), o2.data_ptr(), z2.data_ptr(),
+                                     h2.data_ptr(), net.err.data_ptr(), 5, st), "infer")
+    dout = torch.as_tensor(rng.normal(size=n_pad), dtype=torch.float32, device="cuda")
+    d1, d2 = torch.zeros_like(z1), torch.zeros_like(z1)
+    net._check(lib.sasb200_mlp_backward(n, n_pad, net._ptrs(net.WTb), net.w_out.data_ptr(),
+                                        dout.data_ptr(), z1.data_ptr(), d1.data_ptr(),
+                                        net.err.data_ptr(), st), "backward")
+    net._check(lib.sasb200_mlp_backward_p(n, n_pad, net.img_t.data_ptr(), net.w_out.data_ptr(),
+                                          dout.data_ptr(), z2.data_ptr(), d2.data_ptr(),
+                                          net.err.data_ptr(), 7, st), "backward_p")
+    net.stream.synchronize()
+    assert net.errors() == 0
+    assert torch.equal(z1, z2) and torch.equal(h1, h2)
+    assert torch.equal(d1, d2)
