@@ -38,8 +38,12 @@ def _save():
         return
     try:
         os.makedirs(os.path.dirname(_FILE), exist_ok=True)
-        with open(_FILE, "w") as fid:
+        # one writer per process (one process per GPU): write aside, then
+        # rename, so readers never see a partial file
+        tmp = "%s.%d.tmp" % (_FILE, os.getpid())
+        with open(tmp, "w") as fid:
             json.dump(_CACHE, fid, indent=0)
+        os.replace(tmp, _FILE)
     except OSError:
         pass
 
