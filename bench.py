@@ -373,6 +373,7 @@ def population_compare(n_sets, stride, dev, tune=True):
     for k, (name, q, pars) in enumerate(pop):
         by.setdefault(name, []).append((k, q, pars))
     t_batch = t_plain = 0.0
+    t_gen_batch = t_gen_plain = 0.0
     worst = 0.0
     tuned = {}
     for name, members in by.items():
@@ -412,10 +413,33 @@ def population_compare(n_sets, stride, dev, tune=True):
             shell = raw[2*nq + 2]/total or 1.0
             iq64 = v[0]/shell*raw[0:2*nq:2]/total + v[1]
             worst = max(worst, float(np.max(np.abs(iq_b - iq64)/np.abs(iq64))))
+        # one fit generation end to end (new host values in, I(q) of every
+        # set out): batched update + graph replay + readback against the
+        # plain path's per-set marshal + upload + launch + readback
+        new = [dict(p, scale=1.01*p.get("scale", 1.0)) for _, p in sets]
+        P.capture()
+        P.update(new)
+        P.replay()
+        P.iq()
+        t0 = time.perf_counter()
+        P.update(new)
+        P.replay()
+        P.iq()
+        t_gen_batch += time.perf_counter() - t0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for (k, _, _, _, _), (q, _), pars in zip(calls, sets, new):
+            # the public call: marshal, upload, launch, wait, read back
+            d, v, _ = marshal(model.info, pars, [q])
+            k.Iq(d, v, 0.0, False)
+        t_gen_plain += time.perf_counter() - t0
     n = len(pop)
     return {"sets": n, "sample": "every %d-th of %d seeded sets" % (stride, n_sets),
             "batched_f32c_sets_per_s": n/t_batch, "plain_f64_sets_per_s": n/t_plain,
             "speedup": t_plain/t_batch, "max_rel_err_vs_f64": worst,
+            "generation_e2e": {"batched_f32c_ms": 1e3*t_gen_batch,
+                               "plain_f64_ms": 1e3*t_gen_plain,
+                               "speedup": t_gen_plain/t_gen_batch},
             "autotuned": tuned}
 
 

@@ -286,15 +286,27 @@ class Population:
             self.graph.replay()
 
     def update(self, pars_list):
-        """New parameter values for the same q vectors and dispersity sizes."""
-        off = 0
-        host = self.h_val.numpy()
-        for k, pars in enumerate(pars_list):
-            details, values = self._marshal(pars, np.zeros(1))
-            if tuple(details.buffer) != self.pd_shape[k]:
+        """New parameter values for the same q vectors and dispersity sizes
+        (the next generation of a fit), marshaled in one pass."""
+        from .pack import bulk_call_args
+        if len(pars_list) != self.n_sets:
+            raise ValueError("expected %d parameter sets, got %d"
+                             % (self.n_sets, len(pars_list)))
+        args = bulk_call_args(self.info, pars_list, "2d" if self.line else "1d")
+        checked = {}
+        for k, (details, values, _) in enumerate(args):
+            shape = checked.get(id(details))
+            if shape is None:
+                if self.line:
+                    _check_line(self.info, details)
+                shape = checked[id(details)] = tuple(details.buffer)
+            if shape != self.pd_shape[k] or values.size != self._val_sizes[k]:
                 raise ValueError("set %d changed its dispersity structure" % k)
-            n = self._val_sizes[k]
-            self.stream.synchronize()
+        # the previous upload may still be reading the pinned buffer
+        self.stream.synchronize()
+        host = self.h_val.numpy()
+        off = 0
+        for (_, values, _), n in zip(args, self._val_sizes):
             host[off:off + n] = values
             off += n
         if self.graph is None:
