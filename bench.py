@@ -559,6 +559,7 @@ def run_surrogate(args, world, rank, local):
     torch.cuda.set_device(dev)
     S, rep = train_and_evaluate(n_train_sets=args.surrogate_sets, nq=1000,
                                 epochs=args.surrogate_epochs,
+                                gate_epochs=args.surrogate_gate_epochs,
                                 n_holdout_sets=args.surrogate_holdout, device=dev)
     op = rep["operating_points"]["0.01"]
     line = {
@@ -588,6 +589,7 @@ def main(argv=None):
     ap.add_argument("--surrogate-sets", type=int, default=50000,
                     help="training parameter sets (x 1000 q each)")
     ap.add_argument("--surrogate-epochs", type=int, default=24)
+    ap.add_argument("--surrogate-gate-epochs", type=int, default=16)
     ap.add_argument("--grid", type=int, default=256,
                     help="q grid edge for cylinder2d (smaller for profiling)")
     ap.add_argument("--no-e2e", action="store_true")
