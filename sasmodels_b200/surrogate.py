@@ -146,7 +146,7 @@ class MLP:
         self.out = torch.empty(n_pad, **f32)
         self.dout = torch.empty(n_pad, **f32)
         self.sq = torch.empty(n_pad, **f32)
-        self.splits = 8
+        self.splits = 32     # split-K of the weight gradients: 64+ CTAs at batch 8192
         self.gW = [torch.empty(self.splits*HID*(NIN if l == 0 else HID), **f32)
                    for l in range(4)]
         self.gb = [torch.empty(HID, **f32) for _ in range(4)]
