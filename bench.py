@@ -519,9 +519,9 @@ def extras(dev):
 
 #: FP64 flops issued per evaluation of each workload's dominant kernel,
 #: from the ncu instruction counters of iq_main (2*DFMA + DADD + DMUL per
-#: thread instruction) divided by the evaluations of the captured launch;
-#: see profiles/.
-FLOPS_PER_EVAL = {"cylinder2d": 160.8}
+#: thread instruction) divided by the evaluations of the captured launch
+#: (profiles/iq_main_cylinder2d.md, profiles/iq_main_magnetic.md).
+FLOPS_PER_EVAL = {"cylinder2d": 160.8, "magnetic": 758.0}
 #: dram read+write bytes of the dominant kernel per launch (ncu): the mesh
 #: table is read once from DRAM and then served from L2; it does not grow
 #: with the number of q points (profiles/iq_main_cylinder2d.md)
@@ -588,7 +588,7 @@ def main(argv=None):
     ap.add_argument("--surrogate-holdout", type=int, default=1500)
     ap.add_argument("--surrogate-sets", type=int, default=50000,
                     help="training parameter sets (x 1000 q each)")
-    ap.add_argument("--surrogate-epochs", type=int, default=24)
+    ap.add_argument("--surrogate-epochs", type=int, default=32)
     ap.add_argument("--surrogate-gate-epochs", type=int, default=16)
     ap.add_argument("--grid", type=int, default=256,
                     help="q grid edge for cylinder2d (smaller for profiling)")
