@@ -202,8 +202,88 @@ def cpu_baseline(config, seconds_hint=None):
     return evals/dt, threads, sample, evals, dt
 
 
+def _reference_sets(jobs, threads):
+    """Run the reference DLL on (model, variant, q, pars, nout) jobs, one
+    set per host thread at a time; returns the wall time."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import refdll
+    from sasmodels_b200 import load_model_info
+    prepared = []
+    for model, variant, q, pars, nout in jobs:
+        info = load_model_info(model)
+        qv = [q] if variant == "Iq" else [q, np.zeros_like(q)]
+        details, values, _ = marshal(info, pars, qv)
+        qi = q if variant == "Iq" else np.column_stack([q, np.zeros_like(q)]).ravel()
+        prepared.append((refdll.load(model), variant, np.ascontiguousarray(qi),
+                         details.buffer, values, nout))
+
+    def one(job):
+        dll, variant, q, det, val, nout = job
+        return dll.call(variant, q, det, val, nout)
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as pool:
+        list(pool.map(one, prepared))
+    return time.perf_counter() - t0
+
+
+def reference_population(stride=255):
+    """Reference DLL param-sets/s on every `stride`-th set of the 4096-set
+    population, sets spread over the host threads."""
+    from sasmodels_b200 import workloads
+    pop = workloads.population(n_sets=4096, seed=1)[::stride]
+    threads = host_threads()
+    jobs = [(name, "Iq", q, pars, 2) for name, q, pars in pop]
+    dt = _reference_sets(jobs, threads)
+    return len(jobs)/dt, threads, "every %d-th of 4096 seeded sets (%d sets)" % (stride, len(jobs))
+
+
+def reference_surrogate(n_sets=16, nq=1000, seed=2):
+    """Reference DLL samples/s of the plain cylinder on held-out-like sets
+    (the surrogate's plain path: 1D orientation average for flag 1, the 2D
+    kernel along qx at theta 90, phi 0 for flag 0)."""
+    from sasmodels_b200.surrogate import model_pars, sample_q, sample_sets
+    rng = np.random.default_rng(seed)
+    sets = sample_sets(n_sets, rng)
+    qs = [sample_q(nq, rng) for _ in range(n_sets)]
+    jobs = []
+    for k in range(n_sets):
+        flag = int(sets["flag"][k])
+        pars = model_pars(sets["radius"][k], sets["length"][k], sets["rpd"][k],
+                          sets["lpd"][k], flag)
+        jobs.append(("cylinder", "Iq" if flag else "Iqxy", qs[k], pars, 2 if flag else 1))
+    threads = host_threads()
+    dt = _reference_sets(jobs, threads)
+    return n_sets*nq/dt, threads, "%d seeded held-out-like sets x %d q" % (n_sets, nq)
+
+
 def run_reference(args, world, rank):
     if rank != 0:
+        return
+    if args.config in ("population", "surrogate"):
+        fn = reference_population if args.config == "population" else reference_surrogate
+        unit = "param-sets/s" if args.config == "population" else "samples/s"
+        vals = []
+        for step in range(args.warmup + args.steps):
+            v, threads, sample = fn()
+            if step >= args.warmup:
+                vals.append(v)
+        value = statistics.median(vals)
+        metric = (METRIC if args.config == "population" else
+                  "surrogate log I(q) samples/s at <=1% log-I error with fallback")
+        line = {
+            "impl": "reference", "metric": metric, "value": value, "unit": unit,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": args.config, "sample": sample,
+                       "parallelism": "host threads, one set per thread"},
+            "cpu_baseline": {"value": value, "unit": unit, "cores": threads,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
         return
     values = []
     for step in range(args.warmup + args.steps):
