@@ -14,7 +14,12 @@ One process per GPU (torch.distributed) for the two ways the path shards:
 
 The first two need no reduction on the data path -- the only collective is
 the final gather of results; the third has one small exchange (nout*nq + 4
-doubles per rank).  The evaluation itself is a callable, the GPU
+doubles per rank).
+
+Surrogate training runs data-parallel: identical replicas, each global
+batch split into equal contiguous slices (`batch_slice`), and one
+all-reduce per step of one flat bucket of the ~200k fp32 gradients plus the
+loss (`allreduce_mean`), so every replica applies the same Adam update.  The evaluation itself is a callable, the GPU
 engine by default, so the host logic here runs (and is tested) with the
 gloo backend on CPU as well as NCCL on GPUs.
 """
@@ -185,3 +190,48 @@ def kernel_mesh_partition(kernel, call_details, values, cutoff=0.0, magnetic=Fal
         nq = kernel.q_input.nq
         raw[order] = total[:nq]
     return raw
+
+
+def batch_slice(start, batch, rank, nranks):
+    """[lo, hi) of this rank's contiguous slice of the global batch
+    [start, start + batch); the slices are equal and cover the batch."""
+    if batch % nranks:
+        raise ValueError("global batch %d does not split over %d ranks" % (batch, nranks))
+    local = batch//nranks
+    return start + rank*local, start + (rank + 1)*local
+
+
+def allreduce_mean(tensors, group=None):
+    """Average a list of fp32 tensors in place over the ranks of `group` with
+    ONE all-reduce of one flat bucket (the surrogate's gradients and loss).
+    Every rank receives the same reduced bits, so replicas that start equal
+    stay equal without a parameter broadcast.  Returns the list."""
+    import torch
+    dist = _dist()
+    if not (dist.is_available() and dist.is_initialized()):
+        return tensors
+    size = dist.get_world_size(group)
+    if size == 1:
+        return tensors
+    flat = torch.cat([t.reshape(-1) for t in tensors])
+    dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
+    flat.div_(size)
+    off = 0
+    for t in tensors:
+        k = t.numel()
+        t.view(-1).copy_(flat[off:off + k])
+        off += k
+    return tensors
+
+
+def broadcast_parameters(net, src=0, group=None):
+    """Copy the surrogate network's fp32 parameters from rank `src` to every
+    rank (and refresh its bf16 copies), so data-parallel replicas start from
+    the same weights whatever their seeds; optimiser moments stay zero."""
+    dist = _dist()
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size(group) == 1:
+        return net
+    for p in net.params:
+        dist.broadcast(p, src, group=group)
+    net._sync_bf16()
+    return net

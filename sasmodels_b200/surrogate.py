@@ -249,24 +249,52 @@ class MLP:
             loss = self.sq[:n].mean()
         return loss, self.gW, self.gb, self.gw, self.gbo
 
-    def train_step(self, x, x_lo, y, n, lr, b1=0.9, b2=0.999, eps=1e-8):
+    def train_step(self, x, x_lo, y, n, lr, b1=0.9, b2=0.999, eps=1e-8, reduce=None):
+        """One Adam step on one batch; returns the loss (a device scalar).
+
+        `reduce`, when given, makes this a data-parallel step: it is called
+        on self.stream with the list from `reduced_gradients` and must
+        average it in place over the replicas (``multigpu.allreduce_mean``:
+        one all-reduce of one flat bucket), after which every replica
+        applies the same update."""
+        if reduce is None:
+            loss, dW, db, gw, gbo = self.gradients(x, x_lo, y, n)
+            self.apply_gradients(dW + db + [gw, gbo], lr, self.splits, b1, b2, eps)
+            return loss
+        grads = self.reduced_gradients(x, x_lo, y, n)
+        with self.torch.cuda.stream(self.stream):
+            reduce(grads)
+        self.apply_gradients(grads[1:], lr, 1, b1, b2, eps)
+        return grads[0][0]
+
+    def reduced_gradients(self, x, x_lo, y, n):
+        """[loss (1 element), dW_1..dW_4, db_1..db_4, dw_out, db_out] of one
+        batch as fp32 device tensors, the weight gradients summed over their
+        split-K partials: the ≈200k numbers a data-parallel step exchanges."""
         loss, dW, db, gw, gbo = self.gradients(x, x_lo, y, n)
+        with self.torch.cuda.stream(self.stream):
+            dW = [g.view(self.splits, -1).sum(0) for g in dW]
+            return [loss.reshape(1).clone()] + dW + [g.clone() for g in db + [gw, gbo]]
+
+    def apply_gradients(self, grads, lr, splits, b1=0.9, b2=0.999, eps=1e-8):
+        """Adam update from [dW_1..dW_4 (each `splits` partials), db_1..db_4,
+        dw_out, db_out], refreshing the bf16 weight copies; on self.stream."""
+        dW, rest = grads[:4], grads[4:]
         self.step_count += 1
         st = self.stream.cuda_stream
         lib = self.lib
         for l in range(4):
             nb = NIN if l == 0 else HID
-            self._check(lib.sasb200_adam(HID*nb, self.splits, dW[l].data_ptr(), self.W[l].data_ptr(),
+            self._check(lib.sasb200_adam(HID*nb, splits, dW[l].data_ptr(), self.W[l].data_ptr(),
                                          self.m[l].data_ptr(), self.v[l].data_ptr(), lr, b1, b2, eps,
                                          self.step_count, self.Wb[l].data_ptr(),
                                          self.WTb[l].data_ptr(), HID, nb, st), "adam")
-        for k, g in enumerate(db + [gw, gbo]):
+        for k, g in enumerate(rest):
             p = self.params[4 + k]
             self._check(lib.sasb200_adam(p.numel(), 1, g.data_ptr(), p.data_ptr(),
                                          self.m[4 + k].data_ptr(), self.v[4 + k].data_ptr(), lr,
                                          b1, b2, eps, self.step_count, None, None, 0, 0, st),
                         "adam")
-        return loss
 
     def features(self, radius, length, rpd, lpd, contrast, q, flag):
         """Compensated bf16 features (hi, lo) [n_pad x 16] on the device from
@@ -457,10 +485,26 @@ class Surrogate:
                                  cols["contrast"], cols["q"], cols["flag"].astype(float))
 
     # ---- training ----------------------------------------------------------
-    def _train(self, net, x_all, xlo_all, t_all, n, epochs, batch, lr, seed, scale, log, what):
+    def _train(self, net, x_all, xlo_all, t_all, n, epochs, batch, lr, seed, scale, log, what,
+               group=None):
         """Adam with cosine decay over shuffled batches of one network, all
-        on its stream; returns the loss per epoch (in target units)."""
+        on its stream; returns the loss per epoch (in target units).
+
+        Given a process group of several ranks (every rank holding the same
+        training arrays and the same seed), each global batch is split into
+        equal contiguous slices, one per rank, and the gradients averaged by
+        one all-reduce per step: data-parallel replicas of the same run."""
+        from .multigpu import allreduce_mean, batch_slice, broadcast_parameters
         torch = self.torch
+        dist = torch.distributed
+        nranks, rank, reduce = 1, 0, None
+        if group is not None:
+            nranks, rank = dist.get_world_size(group), dist.get_rank(group)
+        if nranks > 1:
+            broadcast_parameters(net, 0, group)
+
+            def reduce(grads):
+                allreduce_mean(grads, group)
         rng = np.random.default_rng(seed)
         steps = max(1, n//batch)
         total = epochs*steps
@@ -469,7 +513,8 @@ class Surrogate:
         for ep in range(epochs):
             perm = torch.as_tensor(rng.permutation(n), device=net.device)
             for s in range(steps):
-                idx = perm[s*batch:(s + 1)*batch]
+                lo, hi = batch_slice(s*batch, batch, rank, nranks)
+                idx = perm[lo:hi]
                 with torch.cuda.stream(net.stream):
                     xb = x_all.index_select(0, idx)
                     xlb = xlo_all.index_select(0, idx)
@@ -477,7 +522,7 @@ class Surrogate:
                 # cosine decay with a short warm-up
                 frac = step/total
                 rate = lr*min(1.0, (step + 1)/200)*0.5*(1 + math.cos(math.pi*frac))
-                loss = net.train_step(xb, xlb, tb, batch, rate)
+                loss = net.train_step(xb, xlb, tb, hi - lo, rate, reduce=reduce)
                 step += 1
             net.stream.synchronize()
             losses.append(float(loss.item())*scale**2)
@@ -487,9 +532,11 @@ class Surrogate:
             raise RuntimeError("tensor-core kernel reported a timeout")
         return losses
 
-    def fit(self, cols, y, epochs=8, batch=8192, lr=2e-3, seed=0, log=None, huber=0.05):
+    def fit(self, cols, y, epochs=8, batch=8192, lr=2e-3, seed=0, log=None, huber=0.05,
+            group=None):
         """Train the network on log I at unit contrast (Huber loss with
-        threshold `huber` in log I)."""
+        threshold `huber` in log I); data-parallel over the ranks of
+        `group` (e.g. ``torch.distributed.group.WORLD``) when given."""
         torch = self.torch
         good = np.isfinite(y)
         cols = {k: v[good] for k, v in cols.items()}
@@ -501,10 +548,10 @@ class Surrogate:
         t_all = torch.as_tensor((y - self.y_mean)/self.y_std, dtype=torch.float32,
                                 device=self.net.device)
         return self._train(self.net, x_all, xlo_all, t_all, n, epochs, batch, lr, seed,
-                           self.y_std, log, "net")
+                           self.y_std, log, "net", group)
 
     def fit_gate(self, cols, y, epochs=16, batch=8192, lr=2e-3, seed=0, log=None, huber=1.0,
-                 window=16):
+                 window=16, group=None):
         """Train the error gate: a second network of the same shape (the same
         tensor-core kernels) that predicts log(envelope + floor) of the
         trained network's |log I error| from the same features, on sets the
@@ -527,7 +574,7 @@ class Surrogate:
         t_all = torch.as_tensor((target - self.g_mean)/self.g_std, dtype=torch.float32,
                                 device=self.net.device)
         self._train(self.gate, x_all, xlo_all, t_all, n, epochs, batch, lr, seed + 1,
-                    self.g_std, log, "gate")
+                    self.g_std, log, "gate", group)
         return err
 
     # ---- inference ----------------------------------------------------------

@@ -255,3 +255,41 @@ def test_tc_pipelined_training_kernels_match(cuda):
     assert net.errors() == 0
     assert torch.equal(z1, z2) and torch.equal(h1, h2)
     assert torch.equal(d1, d2)
+
+
+@pytest.mark.gpu
+def test_tc_data_parallel_replicas(cuda):
+    """Two replicas each taking half of a global batch, their gradients
+    averaged as the data-parallel all-reduce does, give the full batch's
+    gradients, and both replicas apply the same update bit for bit."""
+    import torch
+    n, half = 2048, 1024
+    a, *_ = _gpu_net(np.random.default_rng(21))
+    b, *_ = _gpu_net(np.random.default_rng(21))
+    full, *_ = _gpu_net(np.random.default_rng(21))
+    rng = np.random.default_rng(22)
+    x, xlo, _, _ = _inputs(rng, n, n)
+    y = torch.as_tensor(rng.normal(0, 1, n), dtype=torch.float32, device="cuda")
+    g_full = full.reduced_gradients(x, xlo, y, n)
+    g_b = b.reduced_gradients(x[half:], xlo[half:], y[half:], half)
+    b.stream.synchronize()
+    seen = {}
+
+    def reduce(grads):
+        for t, u in zip(grads, g_b):
+            t.add_(u).div_(2.0)
+        seen["grads"] = grads
+    loss = a.train_step(x[:half], xlo[:half], y[:half], half, 1e-3, reduce=reduce)
+    a.stream.synchronize()
+    b.apply_gradients(seen["grads"][1:], 1e-3, 1)
+    b.stream.synchronize()
+    full.stream.synchronize()
+    assert a.errors() == 0 and b.errors() == 0 and full.errors() == 0
+    for u, v in zip(seen["grads"], g_full):
+        rel = (torch.linalg.norm(u - v)/torch.linalg.norm(v)).item()
+        assert rel < 1e-4, rel
+    assert abs(loss.item() - g_full[0].item()) < 1e-5*abs(g_full[0].item())
+    for p, q in zip(a.params, b.params):
+        assert torch.equal(p, q)
+    for p, q in zip(a.Wb + a.WTb, b.Wb + b.WTb):
+        assert torch.equal(p, q)

@@ -119,3 +119,82 @@ def test_mesh_ranges_cover():
         rg = mesh_ranges(n, r)
         assert rg[0][0] == 0 and rg[-1][1] == n
         assert all(a[1] == b[0] for a, b in zip(rg[:-1], rg[1:]))
+
+
+def _dp_worker(rank, size, port, queue):
+    sys.path.insert(0, ROOT)
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=size)
+    try:
+        from sasmodels_b200 import multigpu
+        # one flat bucket of several shapes (the loss, matrices, vectors)
+        gen = torch.Generator().manual_seed(rank)
+        grads = [torch.full((1,), float(rank + 1)), torch.arange(6.0).reshape(2, 3)*(rank + 1),
+                 torch.randn(5, generator=gen)]
+        multigpu.allreduce_mean(grads)
+
+        class Net:
+            synced = False
+
+            def _sync_bf16(self):
+                self.synced = True
+        net = Net()
+        net.params = [torch.randn(3, 4, generator=torch.Generator().manual_seed(10 + rank))]
+        multigpu.broadcast_parameters(net)
+        # data-parallel gradient descent of a least-squares model: each rank
+        # takes its slice of every global batch, gradients averaged per step
+        data = torch.Generator().manual_seed(99)
+        X = torch.randn(64, 3, generator=data, dtype=torch.float64)
+        y = torch.randn(64, generator=data, dtype=torch.float64)
+        w = torch.zeros(3, dtype=torch.float64)
+        for step in range(4):
+            lo, hi = multigpu.batch_slice(step*16, 16, rank, size)
+            r = X[lo:hi] @ w - y[lo:hi]
+            g = 2.0*X[lo:hi].T @ r/(hi - lo)
+            multigpu.allreduce_mean([g])
+            w -= 0.1*g
+        queue.put((rank, [t.tolist() for t in grads], net.params[0].tolist(), net.synced,
+                   w.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_data_parallel_helpers_two_ranks():
+    import torch
+    from sasmodels_b200.multigpu import batch_slice
+    ctx = mp.get_context("spawn")
+    queue = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_dp_worker, args=(r, 2, port, queue)) for r in range(2)]
+    for p in procs:
+        p.start()
+    results = sorted(queue.get(timeout=300) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    expect = [[1.5], (torch.arange(6.0).reshape(2, 3)*1.5).tolist(),
+              ((torch.randn(5, generator=torch.Generator().manual_seed(0))
+                + torch.randn(5, generator=torch.Generator().manual_seed(1)))/2).tolist()]
+    data = torch.Generator().manual_seed(99)
+    X = torch.randn(64, 3, generator=data, dtype=torch.float64)
+    y = torch.randn(64, generator=data, dtype=torch.float64)
+    w = torch.zeros(3, dtype=torch.float64)
+    for step in range(4):
+        Xb, yb = X[step*16:(step + 1)*16], y[step*16:(step + 1)*16]
+        w -= 0.1*(2.0*Xb.T @ (Xb @ w - yb)/16)
+    params0 = torch.randn(3, 4, generator=torch.Generator().manual_seed(10)).tolist()
+    for rank, grads, params, synced, w_dp in results:
+        for a, b in zip(grads, expect):
+            np.testing.assert_allclose(np.array(a), np.array(b), rtol=1e-6)
+        assert params == params0 and synced
+        np.testing.assert_allclose(w_dp, w.numpy(), rtol=1e-12, atol=1e-15)
+    # every rank holds the same bits after the reduction
+    assert results[0][1] == results[1][1] and results[0][4] == results[1][4]
+    # the slices of a global batch are equal and cover it
+    assert [batch_slice(32, 16, r, 4) for r in range(4)] == [(32, 36), (36, 40), (40, 44),
+                                                            (44, 48)]
+    with pytest.raises(ValueError):
+        batch_slice(0, 10, 0, 4)
