@@ -448,13 +448,14 @@ def population_compare(n_sets, stride, dev, tune=True):
     import torch
     from sasmodels_b200 import autotune, load_model, workloads
     from sasmodels_b200.batch import Population
+    from sasmodels_b200.pack import columns_from_sets
     pop = workloads.population(n_sets=n_sets, seed=1)[::stride]
     by = {}
     for k, (name, q, pars) in enumerate(pop):
         by.setdefault(name, []).append((k, q, pars))
     t_batch = t_plain = 0.0
-    t_gen_batch = t_gen_plain = 0.0
-    worst = 0.0
+    t_gen_batch = t_gen_plain = t_gen_cols = 0.0
+    worst = cols_diff = 0.0
     tuned = {}
     for name, members in by.items():
         sets = [(q, p) for _, q, p in members]
@@ -513,13 +514,34 @@ def population_compare(n_sets, stride, dev, tune=True):
             d, v, _ = marshal(model.info, pars, [q])
             k.Iq(d, v, 0.0, False)
         t_gen_plain += time.perf_counter() - t0
+        # the same generation given as parameter columns (a fit population
+        # as the optimiser holds it): the table is expanded into the values
+        # vectors on the device inside the replayed graph
+        cols0 = columns_from_sets(P.info, [p for _, p in sets])
+        cols1 = columns_from_sets(P.info, new)
+        PC = Population.from_columns(name, [q for q, _ in sets], cols0, form="float32c",
+                                     device=dev, warps=warps, items_per_warp=ipw)
+        PC.capture()
+        PC.update_columns(cols1)
+        PC.replay()
+        PC.iq()
+        t0 = time.perf_counter()
+        PC.update_columns(cols1)
+        PC.replay()
+        iq_cols = PC.iq()
+        t_gen_cols += time.perf_counter() - t0
+        for a, b in zip(iq_cols, P.iq()):
+            cols_diff = max(cols_diff, float(np.max(np.abs(a - b)/np.abs(b))))
     n = len(pop)
     return {"sets": n, "sample": "every %d-th of %d seeded sets" % (stride, n_sets),
             "batched_f32c_sets_per_s": n/t_batch, "plain_f64_sets_per_s": n/t_plain,
             "speedup": t_plain/t_batch, "max_rel_err_vs_f64": worst,
             "generation_e2e": {"batched_f32c_ms": 1e3*t_gen_batch,
                                "plain_f64_ms": 1e3*t_gen_plain,
-                               "speedup": t_gen_plain/t_gen_batch},
+                               "speedup": t_gen_plain/t_gen_batch,
+                               "columns_ms": 1e3*t_gen_cols,
+                               "columns_speedup": t_gen_plain/t_gen_cols,
+                               "columns_max_rel_diff": cols_diff},
             "autotuned": tuned}
 
 
@@ -665,7 +687,9 @@ def main(argv=None):
                     choices=["cylinder2d", "sphere1d", "magnetic", "surrogate", "population"])
     ap.add_argument("--pop-stride", type=int, default=7,
                     help="population config: evaluate every n-th of the 4096 sets")
-    ap.add_argument("--surrogate-holdout", type=int, default=1500)
+    ap.add_argument("--surrogate-holdout", type=int, default=3000,
+                    help="held-out sets x 1000 q: two thirds calibrate the gate, "
+                         "one third (1e6 samples) is measured")
     ap.add_argument("--surrogate-sets", type=int, default=50000,
                     help="training parameter sets (x 1000 q each)")
     ap.add_argument("--surrogate-epochs", type=int, default=32)

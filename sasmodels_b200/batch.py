@@ -23,6 +23,7 @@ items are issued longest first.
 """
 
 import ctypes as ct
+import os
 
 import numpy as np
 
@@ -49,13 +50,19 @@ def _rmax(model, pars, info):
     rule, as the model's Fq does)."""
     p = dict(info.parameters.defaults)
     p.update({k: v for k, v in pars.items() if k in p})
+    return float(_rmax_arrays(model, p))
+
+
+def _rmax_arrays(model, p):
+    """`_rmax` of parameter values that may be arrays over sets."""
     if model == "ellipsoid":
-        return max(p["radius_polar"], p["radius_equatorial"])
+        return np.maximum(p["radius_polar"], p["radius_equatorial"])
     if model == "core_shell_cylinder":
-        return max(p["radius"] + p["thickness"], 0.5*p["length"] + p["thickness"])
+        return np.maximum(np.add(p["radius"], p["thickness"]),
+                          np.add(0.5*np.asarray(p["length"]), p["thickness"]))
     if model == "cylinder":
-        return max(p["radius"], 0.5*p["length"])
-    return 0.0
+        return np.maximum(p["radius"], 0.5*np.asarray(p["length"]))
+    return np.zeros(())
 
 
 def rule_points(qr):
@@ -96,10 +103,46 @@ def host_pack(model, info, sets, line=False, warps=8, items_per_warp=8, sms=148)
         for d in {id(a[0]): a[0] for a in args}.values():
             _check_line(info, d)
     n = len(sets)
-    nq = np.array([q.size for q in qs], np.int64)
     num_eval = np.array([a[0].num_eval for a in args], np.int64)
-    det_sizes = np.array([a[0].buffer.size for a in args], np.int64)
+    det_all = (np.concatenate([a[0].buffer for a in args]).astype(np.int32) if n
+               else np.zeros(0, np.int32))
     val_sizes = np.array([a[1].size for a in args], np.int64)
+    rmax = np.array([_rmax(model, p, info) for _, p in sets]) if n else np.zeros(0)
+    h = _layout(qs, num_eval, det_all, val_sizes, rmax, line, warps, items_per_warp, sms)
+    h.update(pd_shape=[tuple(a[0].buffer) for a in args],
+             val=np.concatenate([a[1] for a in args]) if n else np.zeros(0))
+    return h
+
+
+def host_pack_columns(model, info, qs, columns, line=False, warps=8, items_per_warp=8, sms=148):
+    """
+    The flat arrays of a population given as parameter columns (see
+    pack.column_args): everything but the values, which the device packer
+    expands from the returned ``columns`` table (host-marshaled values only
+    for the sets the table cannot describe).
+    """
+    from .pack import column_args
+    qs = [np.ascontiguousarray(q, 'd').ravel() for q in qs]
+    n = len(qs)
+    ca = column_args(info, n, columns, "2d" if line else "1d")
+    if line:
+        for d in {id(d): d for d in ca["details"]}.values():
+            _check_line(info, d)
+    p = dict(info.parameters.defaults)
+    names = set(par.name for par in info.parameters.call_parameters)
+    p.update({k: np.asarray(v, float) for k, v in columns.items() if k in names})
+    rmax = np.broadcast_to(_rmax_arrays(model, p), (n,)).astype(float)
+    h = _layout(qs, ca["num_eval"], ca["det"].ravel(), ca["val_sizes"], rmax, line, warps,
+                items_per_warp, sms)
+    h.update(pd_shape=[tuple(r) for r in ca["det"]], val=None, columns=ca)
+    return h
+
+
+def _layout(qs, num_eval, det_all, val_sizes, rmax, line, warps, items_per_warp, sms):
+    """Set descriptors, concatenated q and the work items of a population."""
+    n = len(qs)
+    nq = np.array([q.size for q in qs], np.int64)
+    det_sizes = np.full(n, det_all.size//n if n else 0, np.int64)
     ntile = (nq + 31)//32
 
     def offsets(sizes):
@@ -108,18 +151,14 @@ def host_pack(model, info, sets, line=False, warps=8, items_per_warp=8, sms=148)
     desc = np.stack([nq, offsets(nq), offsets(det_sizes), offsets(val_sizes), num_eval,
                      offsets(2*nq + 4), offsets(nq), offsets(ntile)], axis=1).astype(np.int32)
     q_all = np.concatenate(qs) if n else np.zeros(0)
-    det_all = (np.concatenate([a[0].buffer for a in args]).astype(np.int32) if n
-               else np.zeros(0, np.int32))
-    val_all = np.concatenate([a[1] for a in args]) if n else np.zeros(0)
     # Gauss rule points per q (one node per q for the line form)
     pts = np.ones(q_all.size)
     if not line and n:
-        rmax = np.repeat(np.array([_rmax(model, p, info) for _, p in sets]), nq)
-        pts = np.where(rmax > 0, rule_points(rmax*q_all), 1.0)
+        r = np.repeat(rmax, nq)
+        pts = np.where(r > 0, rule_points(r*q_all), 1.0)
     items, tile_off, tile_items = cut_items(nq, num_eval, pts, warps, items_per_warp, sms)
     return dict(nq=[int(v) for v in nq], num_eval=[int(v) for v in num_eval],
-                pd_shape=[tuple(a[0].buffer) for a in args], val_sizes=list(val_sizes),
-                desc=desc, q=q_all, det=det_all, val=val_all, items=items,
+                val_sizes=list(val_sizes), desc=desc, q=q_all, det=det_all, items=items,
                 tile_off=tile_off, tile_items=tile_items, n_tiles=int(ntile.sum()),
                 n_items=len(items), raw_size=int((2*nq + 4).sum()), iq_size=int(nq.sum()))
 
@@ -180,11 +219,87 @@ def _batch_fn(model):
     return fn, err
 
 
+def _pack_lib():
+    path = os.path.join(_abi.LIB_DIR, "libsasb200_pack.so")
+    if not os.path.exists(path):
+        raise RuntimeError("device packer not built: %s" % path)
+    lib = ct.CDLL(path)
+    P, I = ct.c_void_p, ct.c_int32
+    lib.sasb200_pack_values.argtypes = [I, I, I] + [P]*8 + [P]
+    lib.sasb200_pack_values.restype = I
+    lib.sasb200_pack_max_pars.restype = I
+    lib.sasb200_pack_last_error.restype = ct.c_char_p
+    return lib
+
+
+class _Packer:
+    """The per-set table of a column population in pinned host memory and on
+    the device, and the launch that expands it into the values vectors
+    (``sasb200_pack_values``); sets marshaled on the host are copied from
+    their own pinned rows."""
+
+    def __init__(self, ca, device, stream):
+        import torch
+        self.torch = torch
+        self.lib = _pack_lib()
+        self.stream = stream
+        n, nvalues = ca["scalars"].shape
+        npars = ca["npts"].shape[1]
+        if npars > self.lib.sasb200_pack_max_pars():
+            raise ValueError("%d kernel parameters exceed the device packer's limit" % npars)
+        self.n, self.nvalues, self.npars = n, nvalues, npars
+        sizes = np.asarray(ca["val_sizes"], np.int64)
+        offs = np.concatenate(([0], np.cumsum(sizes)[:-1])).astype(np.int64)
+        self.offs = offs
+        dev_off = offs.copy()
+        host_rows = sorted(ca["host_values"])
+        dev_off[host_rows] = -1
+        f64 = dict(dtype=torch.float64)
+        self.h_table = torch.empty(n*(nvalues + 2*npars), **f64).pin_memory()
+        self.d_table = torch.empty_like(self.h_table, device=device)
+        self.d_npts = torch.as_tensor(ca["npts"].ravel(), device=device)
+        self.d_flags = torch.as_tensor(ca["flags"], device=device)
+        self.d_off = torch.as_tensor(dev_off, device=device)
+        self.d_size = torch.as_tensor(sizes, device=device)
+        self.h_rows = {r: torch.empty(int(sizes[r]), **f64).pin_memory() for r in host_rows}
+
+    def load(self, ca):
+        """Write a table (same structure) into the pinned buffers."""
+        t = self.h_table.numpy()
+        a = self.n*self.nvalues
+        b = a + self.n*self.npars
+        t[:a] = ca["scalars"].ravel()
+        t[a:b] = ca["widths"].ravel()
+        t[b:] = ca["nsigmas"].ravel()
+        for r, buf in self.h_rows.items():
+            buf.numpy()[:] = ca["host_values"][r]
+
+    def enqueue(self, d_val):
+        """Copy the table to the device and expand it into d_val, on the
+        stream (graph-capturable)."""
+        torch = self.torch
+        with torch.cuda.stream(self.stream):
+            self.d_table.copy_(self.h_table, non_blocking=True)
+            for r, buf in self.h_rows.items():
+                o = int(self.offs[r])
+                d_val[o:o + buf.numel()].copy_(buf, non_blocking=True)
+        a = self.n*self.nvalues
+        b = a + self.n*self.npars
+        base = self.d_table.data_ptr()
+        status = self.lib.sasb200_pack_values(
+            self.n, self.nvalues, self.npars, base, base + 8*a, base + 8*b,
+            self.d_npts.data_ptr(), self.d_flags.data_ptr(), self.d_off.data_ptr(),
+            self.d_size.data_ptr(), d_val.data_ptr(), self.stream.cuda_stream)
+        if status != 0:
+            raise RuntimeError("pack_values failed (%d): %s"
+                               % (status, self.lib.sasb200_pack_last_error().decode()))
+
+
 class Population:
     """A packed population of one model on one GPU (see module doc)."""
 
     def __init__(self, model, sets, form="float32c", device=None, cutoff=0.0,
-                 reff_mode=0, warps=8, blocks=0, items_per_warp=8, line=False):
+                 reff_mode=0, warps=8, blocks=0, items_per_warp=8, line=False, columns=None):
         import torch
         self.torch = torch
         self.model = model
@@ -210,7 +325,21 @@ class Population:
         self.stream = torch.cuda.Stream(self.device)
         self.fn, self.err = _batch_fn(model)
         self.graph = None
-        self._pack(sets)
+        self.columns = None
+        if columns is None:
+            self._pack(sets)
+        else:
+            self._pack_columns(sets, columns)
+
+    @classmethod
+    def from_columns(cls, model, qs, columns, **kwargs):
+        """A population given as parameter columns over the q vectors `qs`:
+        `columns` maps parameter names (and ``<name>_pd``, ``_pd_n``,
+        ``_pd_nsigma``, ``_pd_type``) to a scalar shared by all sets or an
+        array with one entry per set.  The values vectors are expanded on
+        the device (``csrc/pack.cu``) from a table of a few numbers per set,
+        and ``update_columns`` refreshes them the same way."""
+        return cls(model, qs, columns=columns, **kwargs)
 
     # ---------------------------------------------------------------- pack --
     def _pack(self, sets):
@@ -218,6 +347,31 @@ class Population:
         sms = torch.cuda.get_device_properties(self.device).multi_processor_count
         h = host_pack(self.model, self.info, sets, self.line, self.warps,
                       self.items_per_warp, sms)
+        self._upload(h)
+        with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+            self.h_val = torch.as_tensor(h["val"]).pin_memory()
+            self.d_val = self.h_val.to(self.device, non_blocking=True)
+        self.stream.synchronize()
+
+    def _pack_columns(self, qs, columns):
+        torch = self.torch
+        sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+        h = host_pack_columns(self.model, self.info, qs, columns, self.line, self.warps,
+                              self.items_per_warp, sms)
+        self._upload(h)
+        ca = h["columns"]
+        self.packer = _Packer(ca, self.device, self.stream)
+        self.h_val = None
+        with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+            self.d_val = torch.empty(max(int(np.sum(ca["val_sizes"])), 1), dtype=torch.float64,
+                                     device=self.device)
+        self.packer.load(ca)
+        self.packer.enqueue(self.d_val)
+        self.columns = ca
+        self.stream.synchronize()
+
+    def _upload(self, h):
+        torch = self.torch
         self.nq = h["nq"]
         self.num_eval = h["num_eval"]
         self.pd_shape = h["pd_shape"]
@@ -230,8 +384,6 @@ class Population:
             self.d_sets = torch.as_tensor(h["desc"].ravel(), **dev)
             self.d_q = torch.as_tensor(h["q"], **dev)
             self.d_det = torch.as_tensor(h["det"], **dev)
-            self.h_val = torch.as_tensor(h["val"]).pin_memory()
-            self.d_val = self.h_val.to(self.device, non_blocking=True)
             self.d_items = torch.as_tensor(h["items"].ravel(), **dev)
             self.d_tile_off = torch.as_tensor(h["tile_off"], **dev)
             self.d_tile_items = torch.as_tensor(h["tile_items"], **dev)
@@ -242,7 +394,6 @@ class Population:
             self.d_iq = torch.empty(h["iq_size"], **f64)
             self.d_counter = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.desc = h["desc"]
-        self.stream.synchronize()
 
     def _marshal(self, pars, q):
         if not self.line:
@@ -274,7 +425,10 @@ class Population:
         self.stream.synchronize()
         g = torch.cuda.CUDAGraph()
         with torch.cuda.device(self.device), torch.cuda.graph(g, stream=self.stream):
-            self.d_val.copy_(self.h_val, non_blocking=True)
+            if self.columns is None:
+                self.d_val.copy_(self.h_val, non_blocking=True)
+            else:
+                self.packer.enqueue(self.d_val)
             self.run()
         self.graph = g
         return g
@@ -285,10 +439,32 @@ class Population:
         with self.torch.cuda.stream(self.stream):
             self.graph.replay()
 
+    def update_columns(self, columns):
+        """New parameter columns for a population made by `from_columns`,
+        with the same q vectors and dispersity sizes: the table is rewritten
+        in pinned memory and expanded on the device by the next `replay()`
+        (or now, on the stream, when no graph was captured)."""
+        from .pack import column_args
+        if self.columns is None:
+            raise ValueError("update_columns needs a population made by from_columns")
+        ca = column_args(self.info, self.n_sets, columns, "2d" if self.line else "1d")
+        old = self.columns
+        if (not np.array_equal(ca["det"], old["det"])
+                or not np.array_equal(ca["val_sizes"], old["val_sizes"])
+                or set(ca["host_values"]) != set(old["host_values"])):
+            raise ValueError("the population changed its dispersity structure")
+        self.stream.synchronize()
+        self.packer.load(ca)
+        self.columns = ca
+        if self.graph is None:
+            self.packer.enqueue(self.d_val)
+
     def update(self, pars_list):
         """New parameter values for the same q vectors and dispersity sizes
         (the next generation of a fit), marshaled in one pass."""
         from .pack import bulk_call_args
+        if self.columns is not None:
+            raise ValueError("a population made by from_columns takes update_columns")
         if len(pars_list) != self.n_sets:
             raise ValueError("expected %d parameter sets, got %d"
                              % (self.n_sets, len(pars_list)))

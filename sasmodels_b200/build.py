@@ -150,7 +150,8 @@ def build_support(force=False):
     return [build_plain("peaks.cu", "libsasb200_peaks.so", force),
             build_plain("mlp.cu", "libsasb200_mlp.so", force,
                         extra_deps=("tc_ptx.cuh",)),
-            build_plain("resolution.cu", "libsasb200_resolution.so", force)]
+            build_plain("resolution.cu", "libsasb200_resolution.so", force),
+            build_plain("pack.cu", "libsasb200_pack.so", force)]
 
 
 def _read(path):

@@ -20,7 +20,7 @@ import numpy as np
 
 from .details import convert_magnetism, make_details
 from .direct_model import RADIUS_MODE_ID, make_call_args
-from .modelinfo import NUM_COMMON_PARS
+from .modelinfo import NUM_COMMON_PARS, NUM_MAGNETIC_PARS
 
 
 def _fields(table, pars, active):
@@ -133,3 +133,137 @@ def bulk_call_args(info, pars_list, dim="1d"):
             magnetic = convert_magnetism(table, values)
             out[i] = (details, values, magnetic)
     return out
+
+
+def _column(columns, name, default, n):
+    """One parameter over the n sets: a scalar broadcast or an array of n."""
+    v = np.asarray(columns.get(name, default))
+    if v.ndim == 0:
+        return np.full(n, v[()])
+    if v.shape != (n,):
+        raise ValueError("column %s has shape %s, expected (%d,)" % (name, v.shape, n))
+    return v
+
+
+def column_args(info, n_sets, columns, dim="1d"):
+    """
+    Marshaling of a population given as parameter columns, for the device
+    packer (``csrc/pack.cu``): `columns` maps parameter names and their
+    dispersity fields (``<name>_pd``, ``_pd_n``, ``_pd_nsigma``,
+    ``_pd_type``) to a scalar shared by every set or an array with one entry
+    per set; parameters not named keep their defaults.
+
+    Returns a dict with the compact per-set table the device expands
+    (``scalars`` [n, nvalues], ``widths``/``nsigmas`` [n, npars], ``npts``
+    [n, npars] with 0 for an idle parameter, ``flags`` [npars]), the
+    ``details`` object, ``det`` buffer, ``num_eval`` and padded ``val_sizes``
+    of every set, and ``host_values`` {set: values} for the sets the table
+    cannot describe (a point clipped at a parameter limit, a dispersity
+    other than gaussian, fewer than 2 points, a zero sigma, a magnetic
+    moment), which ``make_call_args`` marshals.  A device-packed set's values
+    equal ``make_call_args``'s except for the exp of its weights (an ulp or
+    two).
+    """
+    table = info.parameters
+    npars = table.npars
+    n = int(n_sets)
+    if any(getattr(p, "length", 1) > 1 for p in table.call_parameters):
+        raise ValueError("%s has vector parameters: marshal it set by set" % info.id)
+    allowed = _allowed(table)
+    columns = {k: v for k, v in columns.items()
+               if not (k == RADIUS_MODE_ID and RADIUS_MODE_ID not in allowed)}
+    extra = set(columns) - allowed
+    if extra:
+        raise TypeError("Unused parameters in call: %s" % ", ".join(sorted(extra)))
+    active = table.pd_1d if dim == "1d" else table.pd_2d
+    call = table.call_parameters
+    scalars = np.empty((n, table.nvalues))
+    for j, p in enumerate(call):
+        scalars[:, j] = _column(columns, p.name, p.default, n).astype(float)
+    kpars = call[NUM_COMMON_PARS:NUM_COMMON_PARS + npars]
+    widths = np.zeros((n, npars))
+    nsigmas = np.full((n, npars), 3.0)
+    npts = np.zeros((n, npars), np.int32)
+    lengths = np.ones((n, npars), np.int64)
+    flags = np.array([(1 if p.relative_pd else 0) | (2 if (p.relative_pd or not p.polydisperse)
+                                                     else 0) for p in kpars], np.int32)
+    host = np.zeros(n, bool)
+    for k, p in enumerate(kpars):
+        if not p.polydisperse:
+            continue
+        nn = _column(columns, p.name + "_pd_n", 0, n).astype(np.int64)
+        w = _column(columns, p.name + "_pd", 0.0, n).astype(float)
+        ns = _column(columns, p.name + "_pd_nsigma", 3.0, n).astype(float)
+        kind = _column(columns, p.name + "_pd_type", "gaussian", n)
+        dispersed = (nn != 0) & (w != 0.0) & (p.name in active)
+        value = scalars[:, NUM_COMMON_PARS + k]
+        sigma = w*value if p.relative_pd else w
+        center = value if p.relative_pd else np.zeros(n)
+        ends = np.stack([center + (-ns)*sigma, center + ns*sigma])
+        lb, ub = p.limits
+        inside = (ends.min(axis=0) >= lb) & (ends.max(axis=0) <= ub)
+        simple = (kind == "gaussian") & (nn >= 2) & (sigma != 0) & inside
+        host |= dispersed & ~simple
+        npts[:, k] = np.where(dispersed, nn, 0)
+        widths[:, k] = np.where(dispersed, w, 0.0)
+        nsigmas[:, k] = ns
+        lengths[:, k] = np.where(dispersed, nn, 1)
+    if table.nmagnetic:
+        mag = scalars[:, table.nvalues - NUM_MAGNETIC_PARS*table.nmagnetic:]
+        host |= np.any(mag[:, ::NUM_MAGNETIC_PARS] != 0.0, axis=1)
+    det_len = 4*table.max_pd + 4
+    det = np.empty((n, det_len), np.int32)
+    num_eval = np.empty(n, np.int64)
+    val_sizes = np.empty(n, np.int64)
+    details = [None]*n
+    host_values = {}
+    dev = np.nonzero(~host)[0]
+    if dev.size:
+        shapes, inverse = np.unique(lengths[dev], axis=0, return_inverse=True)
+        inverse = inverse.ravel()
+        for g, length in enumerate(shapes):
+            offset = np.cumsum(np.hstack((0, length)))
+            d = make_details(info, length, offset[:-1], offset[-1])
+            rows = dev[inverse == g]
+            data_len = table.nvalues + 2*int(length.sum())
+            det[rows] = d.buffer
+            num_eval[rows] = d.num_eval
+            val_sizes[rows] = data_len + (32 - data_len % 32) % 32
+            for r in rows:
+                details[r] = d
+    q_dummy = [np.zeros(1)] if dim == "1d" else [np.zeros(1), np.zeros(1)]
+    for r in np.nonzero(host)[0]:
+        pars = {}
+        for k, v in columns.items():
+            v = np.asarray(v)
+            v = v[()] if v.ndim == 0 else v[r]
+            pars[k] = v.item() if hasattr(v, "item") else v
+        d, values, _ = make_call_args(info, pars, q_dummy)
+        det[r] = d.buffer
+        num_eval[r] = d.num_eval
+        val_sizes[r] = values.size
+        details[r] = d
+        host_values[int(r)] = values
+    return dict(scalars=scalars, widths=widths, nsigmas=nsigmas, npts=npts, flags=flags,
+                lengths=lengths, details=details, det=det, num_eval=num_eval,
+                val_sizes=val_sizes, host_values=host_values)
+
+
+def columns_from_sets(info, pars_list):
+    """Parameter columns of a list of parameter dicts (for column_args):
+    every name any set gives, with the parameter's default where a set
+    leaves it out."""
+    defaults = info.parameters.defaults
+    names = sorted(set().union(*[set(p) for p in pars_list])) if pars_list else []
+    cols = {}
+    for k in names:
+        if k in defaults:
+            fill = defaults[k]
+        elif k.endswith("_pd_type"):
+            fill = "gaussian"
+        else:
+            fill = 3.0 if k.endswith("_pd_nsigma") else 0.0
+        vals = [p.get(k, fill) for p in pars_list]
+        cols[k] = (np.array(vals, dtype=object) if k.endswith("_pd_type")
+                   else np.array(vals, dtype=float))
+    return cols

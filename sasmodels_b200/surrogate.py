@@ -378,6 +378,21 @@ def model_pars(R, L, rpd, lpd, flag):
     return p
 
 
+def model_columns(sets, idx, flag):
+    """`model_pars` of the sets `idx` as parameter columns (a width of 0
+    leaves the parameter without dispersity, as model_pars omits it)."""
+    cols = dict(radius=np.asarray(sets["radius"], float)[idx],
+                length=np.asarray(sets["length"], float)[idx], sld=1.0, sld_solvent=0.0,
+                scale=1.0, background=0.0,
+                radius_pd=np.maximum(np.asarray(sets["rpd"], float)[idx], 0.0),
+                radius_pd_n=PD_N, radius_pd_nsigma=3.0,
+                length_pd=np.maximum(np.asarray(sets["lpd"], float)[idx], 0.0),
+                length_pd_n=PD_N, length_pd_nsigma=3.0)
+    if not flag:
+        cols.update(theta=90.0, phi=0.0)
+    return cols
+
+
 def plain_unit_iq(sets, qs, device=None, form="float32c", shape=None):
     """I(q) at unit contrast from the plain engines, one array per set, both
     through the batched engine: flag 1 as the 1D orientation average, flag 0
@@ -389,15 +404,16 @@ def plain_unit_iq(sets, qs, device=None, form="float32c", shape=None):
     pops = []
     # both populations are packed and enqueued before either is read back,
     # so the host packing of the second overlaps the first one's kernels
+    flags = np.asarray(sets["flag"]).astype(bool)
     for flag in (1, 0):
-        idx = [k for k in range(n) if bool(sets["flag"][k]) == bool(flag)]
-        if not idx:
+        idx = np.nonzero(flags == bool(flag))[0]
+        if not idx.size:
             continue
-        members = [(qs[k], model_pars(sets["radius"][k], sets["length"][k], sets["rpd"][k],
-                                      sets["lpd"][k], flag)) for k in idx]
         warps, ipw = (shape or {}).get(flag, (8, 8))
-        pop = Population("cylinder", members, form=form, device=device, line=not flag,
-                         warps=warps, items_per_warp=ipw)
+        pop = Population.from_columns("cylinder", [qs[k] for k in idx],
+                                      model_columns(sets, idx, flag), form=form,
+                                      device=device, line=not flag, warps=warps,
+                                      items_per_warp=ipw)
         pop.run()
         pops.append((idx, pop))
     for idx, pop in pops:

@@ -301,15 +301,17 @@ def test_host_pack_population(line):
     assert len(lst) == len(items) == len(set(lst.tolist()))
 
 
-@pytest.mark.parametrize("lib_name", ["mlp", "peaks", "resolution"])
+@pytest.mark.parametrize("lib_name", ["mlp", "peaks", "resolution", "pack"])
 def test_support_libraries_export_header_symbols(lib_name):
-    """libsasb200_{mlp,peaks,resolution}.so load without a GPU and export
-    every function their header (include/sasb200_mlp.h,
-    include/sasb200_resolution.h) declares for them."""
-    header = "sasb200_resolution.h" if lib_name == "resolution" else "sasb200_mlp.h"
+    """libsasb200_{mlp,peaks,resolution,pack}.so load without a GPU and
+    export every function their header (include/sasb200_mlp.h,
+    include/sasb200_resolution.h, include/sasb200_pack.h) declares for
+    them."""
+    header = ("sasb200_%s.h" % lib_name if lib_name in ("resolution", "pack")
+              else "sasb200_mlp.h")
     text = open(os.path.join(ROOT, "include", header)).read()
     names = sorted(set(re.findall(r"\b(sasb200_\w+)\(", text)))
-    want = (names if lib_name == "resolution" else
+    want = (names if lib_name in ("resolution", "pack") else
             [n for n in names if n.startswith("sasb200_probe") == (lib_name == "peaks")])
     assert want
     lib = ct.CDLL(os.path.join(_abi.LIB_DIR, "libsasb200_%s.so" % lib_name))
