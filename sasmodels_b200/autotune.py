@@ -52,9 +52,30 @@ def _size_class(n):
     return int(np.ceil(np.log2(max(n, 1))))
 
 
+_NAMES = {}
+
+
 def _device_name(device):
     import torch
-    return torch.cuda.get_device_name(device)
+    index = torch.device(device).index if not isinstance(device, int) else device
+    if index is None:
+        index = torch.cuda.current_device()
+    if index not in _NAMES:
+        _NAMES[index] = torch.cuda.get_device_name(index)
+    return _NAMES[index]
+
+
+def _tile_key(kernel, variant, n_mesh):
+    return "|".join(["tile", _device_name(kernel.device), kernel.info.id, kernel.lib.name,
+                     variant, str(_size_class(kernel.q_input.nq)), str(_size_class(n_mesh))])
+
+
+def cached_tile(kernel, variant, n_mesh):
+    """The tile code `tune_kernel` chose for this call shape (this device,
+    model, variant and size class), in this process or an earlier one whose
+    cache file is shared; 0 (the library's choice) when there is none."""
+    _load()
+    return int(_CACHE.get(_tile_key(kernel, variant, n_mesh), 0))
 
 
 def _time_stream(fn, stream, reps=2):
@@ -88,26 +109,28 @@ def tune_kernel(kernel, variant, details_dev, values_dev, n_mesh, reps=2, budget
     return it."""
     import torch
     _load()
-    key = "|".join(["tile", _device_name(kernel.device), kernel.info.id,
-                    kernel.lib.name, variant, str(_size_class(kernel.q_input.nq)),
-                    str(_size_class(n_mesh))])
+    key = _tile_key(kernel, variant, n_mesh)
     if key in _CACHE:
         kernel.tile = int(_CACHE[key])
         return kernel.tile
     sms = torch.cuda.get_device_properties(kernel.device).multi_processor_count
     best, best_t = 0, float("inf")
     t_start = time.perf_counter()
-    for code in [0] + tile_candidates(kernel.lib, kernel.q_input.nq, n_mesh, sms):
-        kernel.tile = code
+    kernel._tuning = True          # code 0 is the library's own choice here
+    try:
+        for code in [0] + tile_candidates(kernel.lib, kernel.q_input.nq, n_mesh, sms):
+            kernel.tile = code
 
-        def call():
-            kernel.launch(variant, details_dev, values_dev, 0, n_mesh, 0.0, 0)
-        with torch.cuda.stream(kernel.stream):
-            t = _time_stream(call, kernel.stream, reps)
-        if t < best_t:
-            best, best_t = code, t
-        if time.perf_counter() - t_start > budget_s:
-            break
+            def call():
+                kernel.launch(variant, details_dev, values_dev, 0, n_mesh, 0.0, 0)
+            with torch.cuda.stream(kernel.stream):
+                t = _time_stream(call, kernel.stream, reps)
+            if t < best_t:
+                best, best_t = code, t
+            if time.perf_counter() - t_start > budget_s:
+                break
+    finally:
+        kernel._tuning = False
     kernel.tile = best
     _CACHE[key] = best
     _save()

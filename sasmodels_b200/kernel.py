@@ -167,8 +167,10 @@ class B200Kernel(_KernelBase):
         self._pin_details = None
         self._dev_values = None
         self._dev_details = None
-        #: tile code handed to the C-ABI (0 = library choice)
+        #: tile code handed to the C-ABI (0 = the autotuner's cached choice
+        #: for this call shape, else the library's)
         self.tile = 0
+        self._tuning = False
         self.lib = model.lib
 
     # ------------------------------------------------------------ staging --
@@ -223,6 +225,10 @@ class B200Kernel(_KernelBase):
                cutoff, radius_effective_mode, result_dev=None, tile=None):
         """Enqueue one driver call on ``self.stream``; all arrays on device."""
         result_dev = self._result_dev if result_dev is None else result_dev
+        if tile is None and self.tile == 0 and not self._tuning:
+            # a tile the autotuner measured for this call shape, if any
+            from .autotune import cached_tile
+            tile = cached_tile(self, variant, pd_stop - pd_start)
         tile = int(self.tile if tile is None else tile)
         ws = self.workspace(variant, pd_stop - pd_start, tile)
         self.lib.call(variant, self.q_input.nq, int(pd_start), int(pd_stop),
