@@ -202,6 +202,40 @@ def cpu_baseline(config, seconds_hint=None):
     return evals/dt, threads, sample, evals, dt
 
 
+def cpu_model():
+    """The host CPU's model name (for the baseline record)."""
+    try:
+        with open("/proc/cpuinfo") as fid:
+            for line in fid:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def cpu_single_thread(config):
+    """Reference DLL on one host thread: the first 1/threads of the bounded
+    sample's q points (the per-thread share of the threaded run)."""
+    from oracle import refdll
+    from sasmodels_b200 import load_model_info
+    (name, qv, pars), _ = sample_workload(config)
+    info = load_model_info(name)
+    details, values, magnetic = marshal(info, pars, qv)
+    dim = '2d' if len(qv) == 2 else '1d'
+    var = "Iq" if dim == '1d' else ("Imagnetic" if magnetic else "Iqxy")
+    nout = 2 if info.have_Fq and dim == '1d' else 1
+    n1 = max(1, len(qv[0])//host_threads())
+    if dim == '1d':
+        q = np.ascontiguousarray(qv[0][:n1])
+    else:
+        q = np.empty(2*n1)
+        q[0::2], q[1::2] = qv[0][:n1], qv[1][:n1]
+    t0 = time.perf_counter()
+    refdll.run_threads(name, var, q, details.buffer, values, nout, 1)
+    return n1*details.num_eval/(time.perf_counter() - t0)
+
+
 def _reference_sets(jobs, threads):
     """Run the reference DLL on (model, variant, q, pars, nout) jobs, one
     set per host thread at a time; returns the wall time."""
@@ -299,7 +333,7 @@ def run_reference(args, world, rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": desc, "sample": sample, "parallelism": "host threads, q-sharded"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
-                         "kind": "reference", "sample": sample},
+                         "kind": "reference", "sample": sample, "cpu": cpu_model()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -410,7 +444,9 @@ def run_b200(args, world, rank, local):
         if world == 1 and not args.no_cpu:
             v, threads, sample, _, _ = cpu_baseline(args.config)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads,
-                                    "kind": "reference", "sample": sample}
+                                    "kind": "reference", "sample": sample,
+                                    "value_1_thread": cpu_single_thread(args.config),
+                                    "cpu": cpu_model()}
         print(json.dumps(line), flush=True)
     return line
 
