@@ -347,7 +347,7 @@ def run_b200(args, world, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     (name, qv, pars), desc = workload(args.config, args.grid)
-    model = load_model(name, device=dev)
+    model = load_model(name, dtype=args.dtype, device=dev)
     kernel = model.make_kernel(qv)
     details, values, magnetic = marshal(model.info, pars, qv)
     variant = kernel.variant(magnetic)
@@ -413,7 +413,7 @@ def run_b200(args, world, rank, local):
     line = None
     if rank == 0:
         fp64_peak = peaks.fp64_tflops()
-        flops_per_eval = FLOPS_PER_EVAL.get(args.config)
+        flops_per_eval = FLOPS_PER_EVAL.get(args.config) if args.dtype == "double" else None
         achieved = None
         if flops_per_eval:
             achieved = flops_per_eval*evals/(ms_per_step*1e-3)/1e12
@@ -421,7 +421,8 @@ def run_b200(args, world, rank, local):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
+            "dtype": "f64" if args.dtype == "double" else "f32 compensated (f64 phases and sums)",
+            "data": "synthetic",
             "config": {"workload": desc, "evals_per_step": evals, "nq": nq,
                        "tile": "0x%08x (autotuned)" % tile if tile else "library default",
                        "mesh": n_mesh, "l2": "flushed (256 MB write) before each timed step",
@@ -436,6 +437,15 @@ def run_b200(args, world, rank, local):
                          "flops_per_eval": flops_per_eval,
                          "traffic": TRAFFIC_PER_STEP.get(args.config)},
         }
+        if args.dtype != "double":
+            mufu = peaks.mufu_tops()
+            ops = MUFU_PER_EVAL.get(args.config)
+            got = ops*evals/(ms_per_step*1e-3)/1e12 if ops else None
+            line["roofline"] = {"bound": "xu", "achieved": got, "peak": mufu,
+                                "unit": "Tops/s", "frac": (got/mufu) if got else None,
+                                "peak_source": "measured live: csrc/peaks.cu MUFU probe",
+                                "mufu_ops_per_eval": ops,
+                                "traffic": TRAFFIC_PER_STEP.get(args.config)}
         s = clocks.summary()
         if s:
             line["clocks"] = s
@@ -660,6 +670,9 @@ def extras(dev):
 #: thread instruction) divided by the evaluations of the captured launch
 #: (profiles/iq_main_cylinder2d.md, profiles/iq_main_magnetic.md).
 FLOPS_PER_EVAL = {"cylinder2d": 160.8, "magnetic": 758.0}
+#: MUFU (XU pipe) thread operations per evaluation of the FP32c form of
+#: iq_main, from the same counters (sm__inst_executed_pipe_xu x 32 / evals)
+MUFU_PER_EVAL = {}
 #: dram read+write bytes of the dominant kernel per launch (ncu): the mesh
 #: table is read once from DRAM and then served from L2; it does not grow
 #: with the number of q points (profiles/iq_main_cylinder2d.md)
@@ -732,6 +745,8 @@ def main(argv=None):
     ap.add_argument("--surrogate-gate-epochs", type=int, default=16)
     ap.add_argument("--grid", type=int, default=256,
                     help="q grid edge for cylinder2d (smaller for profiling)")
+    ap.add_argument("--dtype", default="double", choices=["double", "float32c"],
+                    help="arithmetic of the timed kernel (cylinder2d, magnetic, sphere1d)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
