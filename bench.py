@@ -439,12 +439,12 @@ def run_b200(args, world, rank, local):
         }
         if args.dtype != "double":
             mufu = peaks.mufu_tops()
-            ops = MUFU_PER_EVAL.get(args.config)
+            ops = XU_OPS_PER_EVAL.get(args.config)
             got = ops*evals/(ms_per_step*1e-3)/1e12 if ops else None
             line["roofline"] = {"bound": "xu", "achieved": got, "peak": mufu,
                                 "unit": "Tops/s", "frac": (got/mufu) if got else None,
                                 "peak_source": "measured live: csrc/peaks.cu MUFU probe",
-                                "mufu_ops_per_eval": ops,
+                                "xu_ops_per_eval": ops,
                                 "traffic": TRAFFIC_PER_STEP.get(args.config)}
         s = clocks.summary()
         if s:
@@ -670,9 +670,11 @@ def extras(dev):
 #: thread instruction) divided by the evaluations of the captured launch
 #: (profiles/iq_main_cylinder2d.md, profiles/iq_main_magnetic.md).
 FLOPS_PER_EVAL = {"cylinder2d": 160.8, "magnetic": 758.0}
-#: MUFU (XU pipe) thread operations per evaluation of the FP32c form of
-#: iq_main, from the same counters (sm__inst_executed_pipe_xu x 32 / evals)
-MUFU_PER_EVAL = {}
+#: XU-pipe (MUFU sin/cos/rcp/rsqrt and conversions) thread operations per
+#: evaluation of the FP32c form of iq_main: ncu's sm__inst_executed_pipe_xu
+#: (51.6 % of a 16-lane-per-clock peak over the elapsed cycles) x 32 lanes
+#: / evaluations of the captured launch (profiles/iq_main_cylinder2d_f32c.md)
+XU_OPS_PER_EVAL = {"cylinder2d": 12.3}
 #: dram read+write bytes of the dominant kernel per launch (ncu): the mesh
 #: table is read once from DRAM and then served from L2; it does not grow
 #: with the number of q points (profiles/iq_main_cylinder2d.md)
