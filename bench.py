@@ -94,10 +94,10 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, tag=""):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_%d.csv" % os.getpid())
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_%d%s.csv" % (os.getpid(), tag))
 
     def __enter__(self):
         try:
@@ -400,15 +400,19 @@ def run_b200(args, world, rank, local):
             k2(details, values, 0.0, magnetic)
             k2.release()
         barrier()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            k2 = model.make_kernel(qhost)
-            k2(details, values, 0.0, magnetic)
-            k2.release()
-        barrier()
-        te = dist_max(time.perf_counter() - t0)
+        with ClockSampler(local, "_e2e") as e2e_clocks:
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                k2 = model.make_kernel(qhost)
+                k2(details, values, 0.0, magnetic)
+                k2.release()
+            barrier()
+            te = dist_max(time.perf_counter() - t0)
         e2e = {"value": world*evals*args.steps/te, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+        s = e2e_clocks.summary()
+        if s:
+            e2e["clocks"] = s
 
     line = None
     if rank == 0:
