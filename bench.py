@@ -89,19 +89,23 @@ def marshal(info, pars, q_vectors):
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """nvidia-smi clock/throttle sampling during the timed region, on the GPU
+    this process runs on (selected by UUID, so a remapped
+    CUDA_VISIBLE_DEVICES still samples the right board).  Samples go to a
+    temporary file that is removed after the summary is read."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index, tag=""):
-        self.gpu = gpu_index
+    def __init__(self, local_device, tag=""):
+        import tempfile
+        self.gpu = gpu_selector(local_device)
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_%d%s.csv" % (os.getpid(), tag))
+        fd, self.path = tempfile.mkstemp(prefix="sasb200_clocks%s_" % tag, suffix=".csv")
+        os.close(fd)
 
     def __enter__(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
@@ -138,10 +142,28 @@ class ClockSampler:
                 for name, flag in zip(names, parts[5:9]):
                     if flag.lower() == "active":
                         reasons.add(name)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "gpu": self.gpu}
+
+
+def gpu_selector(local_device):
+    """nvidia-smi -i argument for torch device `local_device`: its UUID
+    ("GPU-..."), which names the same board whatever CUDA_VISIBLE_DEVICES
+    remaps; the ordinal only when the UUID is unavailable."""
+    try:
+        import torch
+        uuid = str(torch.cuda.get_device_properties(local_device).uuid)
+        if uuid:
+            return uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+    except Exception:
+        pass
+    return str(local_device)
 
 
 def dist_setup(n_gpus):

@@ -90,9 +90,11 @@ SASB200_DECLARE_MODEL(cylinder)
  * loops).  Same arguments as sasb200_cylinder_Iqxy without workspace and
  * workspace_bytes; the scratch comes from a static 8 MiB device array in the
  * library (SASB200_NOALLOC_SCRATCH_BYTES), held on every GPU that loads the
- * library until the process exits.  The first call on each device looks up
- * the array's device address (cudaGetSymbolAddress, may load the module):
- * make it before any stream capture.  Problems whose scratch for one
+ * library until the process exits.  Every call looks up the array's device
+ * address in the current context (cudaGetSymbolAddress; nothing is cached,
+ * so a device reset between calls is harmless).  The first lookup on a
+ * device may load the module: make the first call on each device before any
+ * stream capture.  Problems whose scratch for one
  * 128-point mesh segment exceeds the array (very large nq) return -2 with a
  * message; larger meshes are processed in chunks.  All calls share the
  * array: calls that overlap on the GPU race, so keep them on one stream.

@@ -27,7 +27,19 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 DEFAULT_MODELS = ["sphere", "cylinder", "core_shell_sphere", "ellipsoid",
                   "core_shell_cylinder"]
-DEFAULT_SASMODELS = "/root/reference"
+
+
+def _default_sasmodels():
+    """$SASMODELS_PATH, a sasmodels checkout beside this repository, or an
+    importable package (sasmodels_b200.build.locate_sasmodels)."""
+    root = os.path.dirname(HERE)
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    from sasmodels_b200.build import locate_sasmodels
+    return locate_sasmodels()
+
+
+DEFAULT_SASMODELS = None
 
 
 def cc():
@@ -40,6 +52,9 @@ def cc():
 
 
 def build(models, sasmodels_path=DEFAULT_SASMODELS, force=False):
+    sasmodels_path = sasmodels_path or _default_sasmodels()
+    if sasmodels_path is None:
+        raise RuntimeError("sasmodels sources not found: set SASMODELS_PATH")
     if sasmodels_path not in sys.path:
         sys.path.insert(0, sasmodels_path)
     os.environ.setdefault("SAS_OPENCL", "none")
@@ -77,6 +92,9 @@ def build(models, sasmodels_path=DEFAULT_SASMODELS, force=False):
 
 def c_models(sasmodels_path=DEFAULT_SASMODELS):
     """Every model plugin with C sources that loads here."""
+    sasmodels_path = sasmodels_path or _default_sasmodels()
+    if sasmodels_path is None:
+        raise RuntimeError("sasmodels sources not found: set SASMODELS_PATH")
     if sasmodels_path not in sys.path:
         sys.path.insert(0, sasmodels_path)
     os.environ.setdefault("SAS_OPENCL", "none")

@@ -106,3 +106,34 @@ def run_threads(name, variant, q, details, values, nout, threads, cutoff=0.0,
         out[nout*lo:nout*hi] = res[:nout*(hi-lo)]
     out[nout*nq:] = parts[0][-4:]
     return out
+
+
+def run_mesh_threads(name, variant, q, details, values, nout, threads, cutoff=0.0,
+                     reff_mode=0):
+    """Mesh-sharded multi-thread evaluation for calls with few q points and a
+    large dispersity mesh: thread k evaluates the contiguous mesh range
+    [pd_start_k, pd_stop_k) into its own zeroed result (the reference's
+    restart contract, kernel_iq.c:381-423), and the partial vectors are added
+    in range order.  Equal to one call up to the rounding of those adds
+    (far below the 1e-12 bar)."""
+    dll = load(name)
+    details = np.ascontiguousarray(details, np.int32)
+    num_eval = int(details[-4])
+    threads = max(1, min(threads, num_eval))
+    bounds = np.linspace(0, num_eval, threads + 1).astype(int)
+    per = 2 if variant != "Iq" else 1
+    nq = np.asarray(q).size//per
+
+    def part(k):
+        res = np.zeros(nout*nq + 4, 'd')
+        if bounds[k] == bounds[k+1]:
+            return res
+        return dll.call(variant, q, details, values, nout, cutoff, reff_mode,
+                        pd_start=int(bounds[k]), pd_stop=int(bounds[k+1]), result=res)
+
+    with ThreadPoolExecutor(max_workers=threads) as pool:
+        parts = list(pool.map(part, range(threads)))
+    out = parts[0].copy()
+    for res in parts[1:]:
+        out += res
+    return out

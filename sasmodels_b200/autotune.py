@@ -66,7 +66,7 @@ def _device_name(device):
 
 
 def _tile_key(kernel, variant, n_mesh):
-    return "|".join(["tile", _device_name(kernel.device), kernel.info.id, kernel.lib.name,
+    return "|".join(["tile", _device_name(kernel.device), kernel.meta.id, kernel.lib.name,
                      variant, str(_size_class(kernel.q_input.nq)), str(_size_class(n_mesh))])
 
 

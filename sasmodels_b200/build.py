@@ -62,9 +62,36 @@ def nvcc_flags(extra=()):
     ] + list(extra)
 
 
+def locate_sasmodels(explicit=None):
+    """
+    Directory that holds the sasmodels plugin package (``<dir>/sasmodels``),
+    or None.  In order: *explicit*; ``$SASMODELS_PATH``; a sasmodels
+    checkout named ``reference`` beside this repository; the directory of an
+    importable ``sasmodels``.  Only the build step and the tests that compare
+    against the reference's own Python code need it; the built libraries run
+    without it.
+    """
+    def ok(d):
+        return bool(d) and os.path.isdir(os.path.join(d, "sasmodels"))
+    for cand in (explicit, os.environ.get("SASMODELS_PATH"),
+                 os.path.join(os.path.dirname(os.path.dirname(PKG)), "reference")):
+        if ok(cand):
+            return os.path.abspath(cand)
+    try:
+        import importlib.util
+        spec = importlib.util.find_spec("sasmodels")
+    except (ImportError, ValueError):
+        spec = None
+    if spec is not None and spec.origin:
+        cand = os.path.dirname(os.path.dirname(spec.origin))
+        if ok(cand):
+            return cand
+    return None
+
+
 def import_sasmodels(path=None):
     """Import the sasmodels plugin package (from *path* if given)."""
-    path = path or os.environ.get("SASMODELS_PATH")
+    path = path or locate_sasmodels()
     if path and path not in sys.path:
         sys.path.insert(0, path)
     os.environ.setdefault("SAS_OPENCL", "none")

@@ -16,10 +16,13 @@
 //     library holds those 8 MiB from when the module is loaded until the
 //     process exits;
 //   * the host cannot pass the array's name to a kernel (in host code it is
-//     only a stand-in, not a device address).  The first call on each device
-//     looks up the device address with cudaGetSymbolAddress, with that device
-//     current, and caches it.  That lookup can load the module, so make the
-//     first call on each device before any stream capture;
+//     only a stand-in, not a device address).  Every call looks up the
+//     device address with cudaGetSymbolAddress, with the caller's device
+//     current, and passes it to the kernels.  Nothing is cached, so a device
+//     reset or a recreated primary context between calls is harmless: the
+//     next call finds the array where the new context put it.  The first
+//     lookup on a device can load the module, so make the first call on each
+//     device before any stream capture;
 //   * no cudaMalloc, cudaFree or allocating library routine is called;
 //   * a problem whose scratch for one 128-point mesh segment exceeds the
 //     array (mainly a very large nq) is rejected with ERR_WORKSPACE and a
@@ -32,7 +35,6 @@
 #pragma once
 
 #include <cstdint>
-#include <mutex>
 #include <cuda_runtime.h>
 
 #define SASB200_NOALLOC_SCRATCH_BYTES (8ull << 20)
@@ -42,33 +44,20 @@ namespace noalloc {
 
 static __device__ __align__(256) unsigned char scratch[SASB200_NOALLOC_SCRATCH_BYTES];
 
-constexpr int MAX_DEVICES = 128;
-
-// Device address of `scratch` on the current device, looked up once per
-// device under a lock.
+// Device address of `scratch` in the current device's context.  Looked up on
+// every call (cheap once the module is loaded), never cached: a cached
+// address would go stale if the caller reset the device or recreated its
+// primary context between calls.
 inline int32_t scratch_address(void **out)
 {
-    static std::mutex lock;
-    static void *addr[MAX_DEVICES] = {};
-    int dev = -1;
-    cudaError_t err = cudaGetDevice(&dev);
-    if (err != cudaSuccess) {
-        std::snprintf(error_buffer(), 256, "cudaGetDevice: %s", cudaGetErrorString(err));
+    void *p = nullptr;
+    const cudaError_t err = cudaGetSymbolAddress(&p, scratch);
+    if (err != cudaSuccess || p == nullptr) {
+        std::snprintf(error_buffer(), 256, "cudaGetSymbolAddress(scratch): %s",
+                      cudaGetErrorString(err));
         return ERR_CUDA;
     }
-    if (dev < 0 || dev >= MAX_DEVICES) return fail(ERR_UNSUPPORTED, "device ordinal out of range");
-    std::lock_guard<std::mutex> guard(lock);
-    if (addr[dev] == nullptr) {
-        void *p = nullptr;
-        err = cudaGetSymbolAddress(&p, scratch);
-        if (err != cudaSuccess || p == nullptr) {
-            std::snprintf(error_buffer(), 256, "cudaGetSymbolAddress(scratch): %s",
-                          cudaGetErrorString(err));
-            return ERR_CUDA;
-        }
-        addr[dev] = p;
-    }
-    *out = addr[dev];
+    *out = p;
     return OK;
 }
 

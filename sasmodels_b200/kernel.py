@@ -108,7 +108,11 @@ class QInput:
 
 
 FP64_NAMES = (None, "double", "d", "float64", np.float64, "double!")
-FP32C_NAMES = ("single", "float", "f", "float32", np.float32, "float32c", "single!", "fast")
+FP32C_NAMES = ("float32c",)
+#: the reference's single-precision names: this backend has no plain FP32
+#: build of the plugin C (generate.convert_type), so these run the
+#: FP32-compensated form, which is more accurate than it, with a warning
+SINGLE_NAMES = ("single", "float", "f", "float32", np.float32, "single!", "fast")
 
 
 class B200Model(_KernelModelBase):
@@ -116,24 +120,43 @@ class B200Model(_KernelModelBase):
     Compute engine for one model on one CUDA device.
 
     *dtype* selects the form: ``"double"`` runs the model plugin's own C in
-    FP64; ``"float32c"`` (also accepted as ``"single"``/``"float32"``, the
-    reference's single-precision names) runs the hand-written FP32-compensated
-    physics where the model has it: FP32 bulk arithmetic, FP64 phases and
-    FP64 sums.  Models without FP32c physics run the FP64 form for either.
-    Results are always float64 arrays.
+    FP64; ``"float32c"`` runs the hand-written FP32-compensated physics where
+    the model has it: FP32 bulk arithmetic, FP64 phases and FP64 sums.
+    The reference's single-precision names (``"single"``, ``"float32"``,
+    ``"fast"``) also select the FP32-compensated form and say so with a
+    ``UserWarning``: it is not the reference's plain FP32 arithmetic
+    (``generate.convert_type``), it is within 1e-5 of FP64.  Models without
+    FP32c physics run the FP64 form for either.  Results are always float64
+    arrays.
+
+    *model_info* is the caller's model description (ours, or a sasmodels
+    ``ModelInfo`` when the model was built through the reference's
+    ``core.build_model``); it is exposed unchanged as ``info``, so callers
+    read their own objects back.  *meta* is this backend's description of
+    the same model (parameter table and library metadata) used internally;
+    it defaults to *model_info*.
     """
-    def __init__(self, model_info, dtype="double", device=None, lib_dir=None):
+    def __init__(self, model_info, dtype="double", device=None, lib_dir=None, meta=None):
         self.info = model_info
+        self.meta = meta if meta is not None else model_info
         if dtype in FP64_NAMES:
             form = "double"
-        elif dtype in FP32C_NAMES:
-            form = "float32c" if model_info.raw.get("f32c") else "double"
+        elif dtype in FP32C_NAMES or dtype in SINGLE_NAMES:
+            form = "float32c" if self.meta.raw.get("f32c") else "double"
+            if dtype in SINGLE_NAMES:
+                import warnings
+                what = ("the FP32-compensated form (FP32 amplitudes with FP64 phases "
+                        "and sums, within 1e-5 of FP64)" if form == "float32c"
+                        else "the FP64 form (no FP32 physics for this model)")
+                warnings.warn("sasmodels_b200: dtype %r runs %s for %s, not the plain "
+                              "single-precision build of the reference"
+                              % (dtype, what, self.meta.id), UserWarning, stacklevel=2)
         else:
             raise ValueError("unsupported dtype %r" % (dtype,))
         self.form = form
         self.dtype = np.dtype('d')
         self.device = device
-        self.lib = _abi.load_library(model_info.id, lib_dir, form)
+        self.lib = _abi.load_library(self.meta.id, lib_dir, form)
 
     def make_kernel(self, q_vectors, reorder=True):
         return B200Kernel(self, q_vectors, reorder=reorder)
@@ -149,6 +172,7 @@ class B200Kernel(_KernelBase):
         torch = _torch()
         self.model = model
         self.info = model.info
+        self.meta = model.meta
         self.dtype = model.dtype
         self.device = _require_cuda(device if device is not None else model.device)
         self.stream = torch.cuda.Stream(self.device)
@@ -156,7 +180,7 @@ class B200Kernel(_KernelBase):
             self.q_input = QInput(q_vectors, self.device, reorder)
             self.dim = '2d' if self.q_input.is_2d else '1d'
             nq = self.q_input.nq
-            nout = 2 if self.info.have_Fq else 1
+            nout = 2 if self.meta.have_Fq else 1
             self.result = np.empty(nq*nout + 4, 'd')
             self._result_dev = torch.zeros(nq*nout + 4, dtype=torch.float64,
                                            device=self.device)
@@ -191,7 +215,7 @@ class B200Kernel(_KernelBase):
         torch = _torch()
         details = np.ascontiguousarray(call_details.buffer, np.int32)
         values = np.ascontiguousarray(values, 'd')
-        validate_call(self.info, details, values)
+        validate_call(self.meta, details, values)
         with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
             pin_d = self._grow("_pin_details", details.size, torch.int32, True)
             pin_v = self._grow("_pin_values", values.size, torch.float64, True)
@@ -271,7 +295,7 @@ class B200Kernel(_KernelBase):
         self._call_kernel(call_details, values, cutoff, magnetic,
                           radius_effective_mode)
         nq = self.q_input.nq
-        nout = 2 if self.info.have_Fq and self.dim == '1d' else 1
+        nout = 2 if self.meta.have_Fq and self.dim == '1d' else 1
         total_weight = self.result[nout*nq + 0]
         if total_weight == 0.:
             total_weight = 1.
@@ -297,7 +321,7 @@ class B200Kernel(_KernelBase):
             res = self.launch(self.variant(magnetic), details_dev, values_dev,
                               0, num_eval, cutoff, 0)
             nq = self.q_input.nq
-            nout = 2 if self.info.have_Fq and self.dim == '1d' else 1
+            nout = 2 if self.meta.have_Fq and self.dim == '1d' else 1
             tail = res[nout*nq:nout*nq + 4]
             total = torch.where(tail[0] == 0, torch.ones_like(tail[0]), tail[0])
             shell = tail[2]/total

@@ -33,16 +33,56 @@ def cylinder_2d(n=256, radius_n=35, length_n=35, theta_n=20, phi_n=20):
     return "cylinder", [qx, qy], pars
 
 
-def cylinder_2d_subgrid(n_sub, n=256):
-    """An n_sub x n_sub block of the cylinder 2D grid (full mesh), taken
-    from the centre of the 256x256 grid; used to time the CPU baseline on a
-    bounded sample and to test parity at full mesh size."""
+def cylinder_2d_subgrid(n_sub, n=256, where="centre"):
+    """An n_sub x n_sub block of the cylinder 2D grid (full mesh), from the
+    centre of the 256x256 grid (|q| <= 0.013 1/A for 8x8: every evaluation
+    takes the small-argument J1 branch) or from its corner (|q| up to
+    0.42 1/A, where qab*R passes 5 and the asymptotic J1 branch runs)."""
     name, (qx, qy), pars = cylinder_2d(n)
     qx = qx.reshape(n, n)
     qy = qy.reshape(n, n)
-    lo = (n - n_sub)//2
+    lo = (n - n_sub)//2 if where == "centre" else 0
     return name, [qx[lo:lo+n_sub, lo:lo+n_sub].ravel(),
                   qy[lo:lo+n_sub, lo:lo+n_sub].ravel()], pars
+
+
+def cylinder_2d_strided(stride, n=256):
+    """Every stride-th row and column of the cylinder 2D grid (full mesh):
+    a sample with the branch mix of the whole grid (16 -> 16x16 points)."""
+    name, (qx, qy), pars = cylinder_2d(n)
+    qx = qx.reshape(n, n)[::stride, ::stride].ravel()
+    qy = qy.reshape(n, n)[::stride, ::stride].ravel()
+    return name, [qx, qy], pars
+
+
+def cylinder_j1_large_fraction(qx, qy, pars):
+    """Fraction of the (q, mesh point) evaluations of the cylinder 2D
+    workload whose J1 argument qab*R exceeds 5, i.e. that take the
+    asymptotic branch of the reference's J1 (models/lib/sas_J1.c).  Computed
+    on the host from the same mesh: orientation jitter (theta, phi) and
+    radius only; length does not enter qab."""
+    from .direct_model import get_mesh
+    from .core import load_model_info
+    info = load_model_info("cylinder")
+    mesh = {p.name: m for p, m in zip(info.parameters.call_parameters,
+                                      get_mesh(info, pars, dim='2d'))}
+    radius = np.asarray(mesh["radius"][1])
+    dtheta = np.asarray(mesh["theta"][1])
+    dphi = np.asarray(mesh["phi"][1])
+    th, ph = np.radians(pars["theta"]), np.radians(pars["phi"])
+    dt, dp = np.meshgrid(np.radians(dtheta), np.radians(dphi), indexing="ij")
+    dt, dp = dt.ravel(), dp.ravel()
+    # third row of the jitter x view rotation (kernel_iq.c qac_rotation)
+    V31, V32 = np.sin(th)*np.cos(ph), np.sin(ph)*np.sin(th)
+    V11, V12 = np.cos(ph)*np.cos(th), np.sin(ph)*np.cos(th)
+    V21, V22 = -np.sin(ph), np.cos(ph)
+    J31, J32, J33 = np.sin(dt), -np.sin(dp)*np.cos(dt), np.cos(dp)*np.cos(dt)
+    R31 = J31*V11 + J32*V21 + J33*V31
+    R32 = J31*V12 + J32*V22 + J33*V32
+    qc = np.outer(qx, R31) + np.outer(qy, R32)
+    qab = np.sqrt(np.maximum((qx**2 + qy**2)[:, None] - qc**2, 0.0))
+    big = (qab[:, :, None]*radius[None, None, :] > 5.0)
+    return float(big.mean())
 
 
 def core_shell_sphere_magnetic(n=128, seed=0, radius_n=51, thickness_n=21):

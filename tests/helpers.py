@@ -57,12 +57,19 @@ def nout_of(info, dim):
     return 2 if info.have_Fq and dim == '1d' else 1
 
 
-def reference_raw(name, info, q_vectors, pars, cutoff=0.0, reff_mode=0, threads=1):
+def reference_raw(name, info, q_vectors, pars, cutoff=0.0, reff_mode=0, threads=1,
+                  split="q"):
+    """Raw result vector of the reference DLL.  With threads > 1 the call is
+    sharded over host threads by q (bitwise equal to one call) or, with
+    split="mesh", by dispersity-mesh range (for few q and a large mesh)."""
     from oracle import refdll
     details, values, magnetic = marshal(info, pars, q_vectors)
     dim = '2d' if len(q_vectors) == 2 else '1d'
     nout = nout_of(info, dim)
     q = interleave(q_vectors)
+    if threads > 1 and split == "mesh":
+        return refdll.run_mesh_threads(name, variant(dim, magnetic), q, details.buffer,
+                                       values, nout, threads, cutoff, reff_mode)
     if threads > 1:
         return refdll.run_threads(name, variant(dim, magnetic), q, details.buffer,
                                   values, nout, threads, cutoff, reff_mode)
@@ -129,3 +136,71 @@ def compare_raw(ours, ref, nout, nq, rtol=RTOL_FP64):
 
 def load_info(name):
     return core.load_model_info(name)
+
+
+def host_threads():
+    """Host threads this process may use (for sharding oracle calls)."""
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+#: members of the 4096-set seeded fit population (workloads.population,
+#: seed 1) at full size, with the q points of each set that the parity tests
+#: evaluate (indices into the set's own q vector; each q is independent):
+#:   1747 core_shell_cylinder, pd 67 x 59 x 68 = 268,804 points; its largest
+#:        q puts 50,451 (q, mesh point) pairs on the 5000-point Gauss rule
+#:   2975 core_shell_cylinder, pd 65 x 66 x 67 = 287,430 points
+#:   3    core_shell_cylinder, pd 55 x 66 x 62 = 225,060 points
+#:   563  core_shell_cylinder, pd 39 on one dimension, 5000-point rule at top q
+#:   924  ellipsoid, pd 65 x 63, 500-point rule at top q
+#:   2584 ellipsoid, pd 71 x 60
+FULL_SIZE_SETS = {1747: 3, 2975: 3, 3: 6, 563: 12, 924: 12, 2584: 12}
+
+
+def full_size_population():
+    """[(index, model, q_subsample, pars)] of FULL_SIZE_SETS: each set's
+    full dispersity mesh at its smallest, largest and evenly spaced q."""
+    import numpy as np
+    from sasmodels_b200 import workloads
+    pop = workloads.population(n_sets=4096, seed=1)
+    out = []
+    for k, nsub in FULL_SIZE_SETS.items():
+        name, q, pars = pop[k]
+        idx = np.unique(np.linspace(0, len(q) - 1, nsub).round().astype(int))
+        out.append((k, name, q[idx], pars))
+    return out
+
+
+_FULL_SIZE_REF = {}
+
+
+def full_size_reference(k, name, q, pars):
+    """Reference DLL raw vector of a FULL_SIZE_SETS member (mesh-sharded over
+    the host threads), computed once per process."""
+    if k not in _FULL_SIZE_REF:
+        _FULL_SIZE_REF[k] = reference_raw(name, load_info(name), [q], pars,
+                                          threads=host_threads(), split="mesh")
+    return _FULL_SIZE_REF[k]
+
+
+def gauss_rule_counts(name, q, pars):
+    """{rule length: number of (q, mesh point) pairs} for a 1D ellipsoid or
+    core_shell_cylinder call: the adaptive Gauss rule each pair uses, chosen
+    from q times the largest dimension of that mesh point
+    (models/lib/adaptive.c gauss_weights; models/ellipsoid.c,
+    models/core_shell_cylinder.c)."""
+    import numpy as np
+    from sasmodels_b200.batch import rule_points
+    info = load_info(name)
+    mesh = {p.name: np.asarray(m[1]) for p, m in
+            zip(info.parameters.call_parameters, get_mesh(info, pars, dim='1d'))}
+    if name == "ellipsoid":
+        r = np.maximum.outer(mesh["radius_polar"], mesh["radius_equatorial"]).ravel()
+    else:
+        r = np.maximum(np.add.outer(mesh["radius"], mesh["thickness"])[:, :, None],
+                       (0.5*mesh["length"])[None, None, :]
+                       + mesh["thickness"][None, :, None]).ravel()
+    n = rule_points(np.outer(q, r))
+    return {int(k): int((n == k).sum()) for k in (20, 76, 500, 5000)}

@@ -12,8 +12,9 @@ class _FakeLib:
 
 
 class _FakeKernel:
-    class info:
+    class meta:
         id = "cylinder"
+    info = meta
 
     class q_input:
         nq = 65536

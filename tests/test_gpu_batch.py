@@ -7,7 +7,9 @@ FP32c at 1e-5; graph capture/replay with new values; determinism.
 import numpy as np
 import pytest
 
-from helpers import RTOL_FP64, compare_raw, load_info, marshal, normalise, reference_raw
+from helpers import (RTOL_FP64, compare_raw, full_size_population,
+                     full_size_reference, load_info, marshal, normalise,
+                     reference_raw)
 from sasmodels_b200 import workloads
 from sasmodels_b200.batch import Population
 
@@ -151,3 +153,25 @@ def test_batch_ragged_sets(cuda):
         ref = reference_raw("ellipsoid", info, [q], pars)
         worst, f2rel = compare_raw(raw, ref, 2, len(q), RTOL_FP64)
         assert worst <= 1.0, (len(q), worst, f2rel)
+
+
+@pytest.mark.parametrize("form, rtol", [("double", RTOL_FP64), ("float32c", 1e-5)])
+def test_batch_full_size_against_reference(cuda, form, rtol):
+    """The batched engine on population members at full size (dispersity
+    meshes up to 287,430 points, the 500- and 5000-point Gauss rules), FP64
+    at the 1e-12 bar and FP32c at 1e-5, raw sums and I(q) against the
+    reference DLL."""
+    by = {}
+    for k, name, q, pars in full_size_population():
+        by.setdefault(name, []).append((k, q, pars))
+    for name, members in by.items():
+        info = load_info(name)
+        pop = Population(name, [(q, p) for _, q, p in members], form=form)
+        pop.run()
+        for (k, q, pars), raw, iq in zip(members, pop.raw(), pop.iq()):
+            ref = full_size_reference(k, name, q, pars)
+            worst, f2rel = compare_raw(raw, ref, 2, len(q), rtol)
+            assert worst <= 1.0, (name, k, form, worst, f2rel)
+            _, values, _ = marshal(info, pars, [q])
+            I_ref = normalise(ref, 2, len(q), values)["I"]
+            np.testing.assert_allclose(iq, I_ref, rtol=max(rtol, 1e-13), atol=0)

@@ -11,9 +11,10 @@ reference harness's 5 significant digits.
 import numpy as np
 import pytest
 
-from helpers import (MODELS, RTOL_FP64, compare_raw, golden, interleave,
-                     is_near, load_info, marshal, normalise, nout_of,
-                     reference_raw, variant)
+from helpers import (FULL_SIZE_SETS, MODELS, RTOL_FP64, compare_raw,
+                     full_size_population, full_size_reference, gauss_rule_counts,
+                     golden, host_threads, interleave, is_near, load_info, marshal,
+                     normalise, nout_of, reference_raw, variant)
 from sasmodels_b200 import direct_model, load_model, workloads
 
 pytestmark = pytest.mark.gpu
@@ -93,6 +94,41 @@ def test_cylinder_2d_full_mesh_subgrid(cuda):
     256x256 grid."""
     name, qv, pars = workloads.cylinder_2d_subgrid(8)
     assert_parity(name, qv, pars)
+
+
+@pytest.mark.parametrize("where", ["corner", "strided"])
+def test_cylinder_2d_full_mesh_off_centre(cuda, where):
+    """cylinder 2D oriented at the full 490000-point mesh away from the grid
+    centre: the corner 8x8 block (|q| up to 0.42 1/A; 56 % of evaluations
+    take the asymptotic J1 branch, x = qab*R > 5, models/lib/sas_J1.c) and a
+    strided 16x16 sample of the whole grid (every 16th row and column; 21 %
+    asymptotic, the branch mix of the full grid).  Here the cancellation in
+    qab^2 = |q|^2 - qc^2 and the J1 large-argument form both run."""
+    if where == "corner":
+        name, qv, pars = workloads.cylinder_2d_subgrid(8, where="corner")
+        least = 0.5
+    else:
+        name, qv, pars = workloads.cylinder_2d_strided(16)
+        least = 0.15
+    assert workloads.cylinder_j1_large_fraction(qv[0], qv[1], pars) > least
+    assert_parity(name, qv, pars, threads=host_threads())
+
+
+@pytest.mark.parametrize("k", list(FULL_SIZE_SETS))
+def test_population_full_size(cuda, k):
+    """Population members at full size (dispersity meshes up to
+    67 x 59 x 68 points, the 500- and 5000-point Gauss rules) through the
+    plain FP64 kernel against the reference DLL, on a q subsample of each
+    set that keeps its smallest and largest q."""
+    (_, name, q, pars), = [c for c in full_size_population() if c[0] == k]
+    rules = gauss_rule_counts(name, q, pars)
+    if k in (1747, 563):
+        assert rules[5000] > 0, rules
+    ours, nout, nq, values = gpu_raw(name, [q], pars)
+    ref = full_size_reference(k, name, q, pars)
+    worst, f2rel = compare_raw(ours, ref, nout, nq)
+    assert worst <= 1.0, "%s set %d: worst err %.3g x tol (max F^2 rel %.3g)" % (
+        name, k, worst, f2rel)
 
 
 def test_magnetic_full_mesh_subgrid(cuda):
