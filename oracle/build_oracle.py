@@ -11,7 +11,13 @@ For each model, writes a C translation unit made of
 
 and compiles it with the reference DLL's flags plus OpenMP into
 ``oracle/_build/liboracle_<model>.so`` (exported: ``oracle_kernel``).
-The generated C stays in the git-ignored build folder.
+
+The same model sources and binding are also compiled as C++ around
+oracle/sasflops.hpp (the SAS-flop counting arithmetic) and
+oracle/sasflops_driver.hpp into ``oracle/_build/libsasflops_<model>.so``
+(exported: ``sasflops_count``), the instrumented restatement that sizes the
+roofline numerator (driven by oracle/sasflops.py).  The generated sources
+stay in the git-ignored build folder.
 
     python oracle/build_oracle.py [model ...] [--sasmodels PATH]
 """
@@ -188,7 +194,25 @@ def build(models, sasmodels_path=DEFAULT_SASMODELS):
         with open(os.path.join(OUT, "oracle_%s.json" % name), "w") as fid:
             json.dump(meta, fid)
         built.append(so)
+        built.append(_build_counter(name, codes, bind))
     return built
+
+
+def _build_counter(name, codes, bind):
+    """The SAS-flop counting library of one model (C++, OpenMP)."""
+    unit = ["#define FLOAT_SIZE 8", '#include "sasflops.hpp"'] + codes + \
+        [bind, '#include "sasflops_driver.hpp"']
+    cpp = os.path.join(OUT, "sasflops_%s.cpp" % name)
+    with open(cpp, "w") as fid:
+        fid.write("\n".join(unit))
+    so = os.path.join(OUT, "libsasflops_%s.so" % name)
+    cmd = ["/usr/bin/g++", "-std=c++17", "-O2", "-fopenmp", "-fPIC", "-shared",
+           "-Wno-unused-function", "-I", HERE, cpp, "-o", so, "-lm"]
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode:
+        raise RuntimeError("SAS-flop counter compile failed for %s:\n%s"
+                           % (name, proc.stderr[-6000:]))
+    return so
 
 
 def main(argv=None):
