@@ -64,7 +64,9 @@ def sample_workload(config):
     """Bounded CPU sample of the same workload (full mesh, fewer q)."""
     from sasmodels_b200 import workloads
     if config == "cylinder2d":
-        return workloads.cylinder_2d_subgrid(32), "32x32 q block of the 256x256 grid, full 490000-point mesh"
+        return (workloads.cylinder_2d_strided(8),
+                "every 8th row and column of the 256x256 grid (32x32 q, the branch mix "
+                "of the whole grid), full 490000-point mesh")
     if config == "sphere1d":
         return workloads.sphere_1d(), "full workload"
     if config == "magnetic":
@@ -219,9 +221,13 @@ def cpu_baseline(config, seconds_hint=None):
     refdll.run_threads(name, var, q[:2*min(threads, len(qv[0]))] if dim == '2d' else q[:threads],
                        details.buffer, values, nout, threads)
     t0 = time.perf_counter()
-    refdll.run_threads(name, var, q, details.buffer, values, nout, threads)
+    raw = refdll.run_threads(name, var, q, details.buffer, values, nout, threads)
     dt = time.perf_counter() - t0
+    cpu_baseline.last[config] = (name, qv, pars, values, nout, raw)
     return evals/dt, threads, sample, evals, dt
+
+
+cpu_baseline.last = {}
 
 
 def cpu_model():
@@ -234,6 +240,34 @@ def cpu_model():
     except OSError:
         pass
     return None
+
+
+def normalised_iq(raw, nout, nq, values):
+    """scale/V_shell * <F^2> + background from a raw result vector
+    (sasmodels/kernel.py:80-188)."""
+    total = raw[nout*nq] or 1.0
+    shell = raw[nout*nq + 2]/total or 1.0
+    return values[0]/shell*raw[0:nout*nq:nout]/total + values[1]
+
+
+def errors_vs_dll(config, dev):
+    """Max relative difference of I(q) from the reference DLL for the FP64
+    and FP32c forms on the bounded sample of `config` that cpu_baseline just
+    timed (the DLL's output is the checker; nothing here is timed)."""
+    from sasmodels_b200 import load_model
+    from sasmodels_b200.direct_model import call_kernel
+    if config not in cpu_baseline.last:
+        cpu_baseline(config)
+    name, qv, pars, values, nout, raw = cpu_baseline.last[config]
+    ref = normalised_iq(raw, nout, len(qv[0]), values)
+    out = {}
+    for dtype in ("double", "float32c"):
+        kernel = load_model(name, dtype=dtype, device=dev).make_kernel(qv)
+        got = call_kernel(kernel, dict(pars))
+        kernel.release()
+        out["max_rel_err_vs_dll_" + ("f64" if dtype == "double" else "f32c")] = \
+            float(np.max(np.abs(got - ref)/np.abs(ref)))
+    return out
 
 
 def cpu_single_thread(config):
@@ -366,20 +400,44 @@ def run_b200(args, world, rank, local):
     import torch
     from sasmodels_b200 import load_model, peaks
 
+    from sasmodels_b200 import multigpu
+
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     (name, qv, pars), desc = workload(args.config, args.grid)
     model = load_model(name, dtype=args.dtype, device=dev)
+    nq_total = len(qv[0])
+    split = args.split == "q" and world > 1
+    if split:
+        # this rank's contiguous block of the image (q partition)
+        lo, hi = multigpu.q_blocks(nq_total, world)[rank]
+        qv = [np.ascontiguousarray(v[lo:hi]) for v in qv]
     kernel = model.make_kernel(qv)
     details, values, magnetic = marshal(model.info, pars, qv)
     variant = kernel.variant(magnetic)
     nq = kernel.q_input.nq
     n_mesh = details.num_eval
     evals = nq*n_mesh
+    evals_all = nq_total*n_mesh if split else world*evals
     dev_d, dev_v = kernel.upload(details, values)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     stream = kernel.stream
-    launches_per_step = 3   # mesh_prepare, iq_main, finalize
+    # mesh_prepare, iq_main, finalize (one fused kernel for a small mesh)
+    launches_per_step = kernel.lib.launches(variant, nq, n_mesh)
+    nout = 2 if model.meta.have_Fq and kernel.dim == '1d' else 1
+
+    def step():
+        """One step on the kernel stream: the evaluation of this rank's
+        share and, for a split image, the all-gather of every rank's block
+        (device tensors, caller's q order) into the whole image."""
+        res = kernel.launch(variant, dev_d, dev_v, 0, n_mesh, 0.0, 0)
+        if split:
+            slots = res[:nout*nq]
+            if kernel.q_input.order_dev is not None:
+                slots = torch.empty_like(slots).index_copy_(0, kernel.q_input.order_dev,
+                                                            slots)
+            return multigpu.gather_blocks(slots)
+        return res
 
     tile = 0
     if not args.no_tune:
@@ -388,7 +446,7 @@ def run_b200(args, world, rank, local):
                                     budget_s=15.0)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
-            kernel.launch(variant, dev_d, dev_v, 0, n_mesh, 0.0, 0)
+            step()
     barrier()
 
     times = []
@@ -401,14 +459,14 @@ def run_b200(args, world, rank, local):
                 start = torch.cuda.Event(enable_timing=True)
                 stop = torch.cuda.Event(enable_timing=True)
                 start.record(stream)
-                kernel.launch(variant, dev_d, dev_v, 0, n_mesh, 0.0, 0)
+                step()
                 stop.record(stream)
                 times.append((start, stop))
         barrier()
         wall = time.perf_counter() - t_wall
     step_s = [a.elapsed_time(b)*1e-3 for a, b in times]
     t_total = dist_max(sum(step_s))
-    value = world*evals*args.steps/t_total
+    value = evals_all*args.steps/t_total
     ms_per_step = 1e3*t_total/args.steps
 
     # end to end through the public API with host buffers
@@ -417,20 +475,27 @@ def run_b200(args, world, rank, local):
         qhost = [np.ascontiguousarray(v) for v in qv]
         h2d = sum(v.nbytes for v in qhost) + details.buffer.nbytes + values.nbytes
         d2h = kernel.result.nbytes
-        for _ in range(1):
+
+        def e2e_step():
+            # the public call on this rank's q points from host arrays, I(q)
+            # back on the host; a split image is then all-gathered so every
+            # rank holds the whole I(q)
             k2 = model.make_kernel(qhost)
-            k2(details, values, 0.0, magnetic)
+            I = k2(details, values, 0.0, magnetic)
             k2.release()
+            if split:
+                I = multigpu.gather_blocks(torch.as_tensor(I)).cpu().numpy()
+            return I
+
+        e2e_step()
         barrier()
         with ClockSampler(local, "_e2e") as e2e_clocks:
             t0 = time.perf_counter()
             for _ in range(args.steps):
-                k2 = model.make_kernel(qhost)
-                k2(details, values, 0.0, magnetic)
-                k2.release()
+                e2e_step()
             barrier()
             te = dist_max(time.perf_counter() - t0)
-        e2e = {"value": world*evals*args.steps/te, "unit": UNIT,
+        e2e = {"value": evals_all*args.steps/te, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
         s = e2e_clocks.summary()
         if s:
@@ -439,29 +504,50 @@ def run_b200(args, world, rank, local):
     line = None
     if rank == 0:
         fp64_peak = peaks.fp64_tflops()
-        flops_per_eval = FLOPS_PER_EVAL.get(args.config) if args.dtype == "double" else None
-        achieved = None
-        if flops_per_eval:
-            achieved = flops_per_eval*evals/(ms_per_step*1e-3)/1e12
+        roofline = {"bound": "fp64", "unit": "TFLOP/s", "peak": fp64_peak,
+                    "peak_source": "measured live: csrc/peaks.cu DFMA probe (of measured)",
+                    "traffic": TRAFFIC_PER_STEP.get(args.config)}
+        sf = SASFLOPS.get(args.config) if args.dtype == "double" else None
+        if sf:
+            per_eval = sf["eval"]/sf["evals"]
+            if sf["evals"] == evals:
+                total = sf["eval"] + sf["point"] + sf["q"]
+                how = "exact count of this configuration"
+            else:
+                total = per_eval*evals
+                how = "per-evaluation mean of the full configuration x evaluations"
+            achieved = total/(ms_per_step*1e-3)/1e12
+            roofline.update({
+                "achieved": achieved, "frac": achieved/fp64_peak,
+                "numerator": "algorithmic SAS-flops: the SAS-flop v1 count of the "
+                             "reference's own model C on this configuration's inputs, "
+                             "every branch replayed (oracle/sasflops.py); " + how,
+                "sasflops_per_step": total, "sasflops_per_eval": per_eval})
+        issued = ISSUED_FP64_PER_EVAL.get(args.config) if args.dtype == "double" else None
+        if issued:
+            got = issued*evals/(ms_per_step*1e-3)/1e12
+            roofline["fp64_pipe"] = {
+                "issued_flops_per_eval": issued, "achieved": got, "frac": got/fp64_peak,
+                "source": "ncu DFMA/DMUL/DADD counts of the current iq_main "
+                          "(2 x DFMA + DMUL + DADD per evaluation)"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong" if split else "weak",
+            "vs_baseline": None,
             "dtype": "f64" if args.dtype == "double" else "f32 compensated (f64 phases and sums)",
             "data": "synthetic",
-            "config": {"workload": desc, "evals_per_step": evals, "nq": nq,
+            "config": {"workload": desc, "evals_per_step": evals_all, "nq": nq_total,
                        "tile": "0x%08x (autotuned)" % tile if tile else "library default",
                        "mesh": n_mesh, "l2": "flushed (256 MB write) before each timed step",
-                       "parallelism": "replicas x%d (one workload per GPU)" % world},
+                       "parallelism": (
+                           "q partition x%d: contiguous q blocks of one image, one per GPU, "
+                           "blocks all-gathered as device tensors inside each step" % world
+                           if split else "replicas x%d (one workload per GPU)" % world)},
             "e2e": e2e,
             "gpu_launches": launches_per_step*args.steps,
             "wall_s": wall,
-            "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak,
-                         "unit": "TFLOP/s",
-                         "frac": (achieved/fp64_peak) if achieved else None,
-                         "peak_source": "measured live: csrc/peaks.cu DFMA probe",
-                         "flops_per_eval": flops_per_eval,
-                         "traffic": TRAFFIC_PER_STEP.get(args.config)},
+            "roofline": roofline,
         }
         if args.dtype != "double":
             mufu = peaks.mufu_tops()
@@ -475,14 +561,15 @@ def run_b200(args, world, rank, local):
         s = clocks.summary()
         if s:
             line["clocks"] = s
-        if world == 1 and not args.no_extras and args.config == "cylinder2d":
-            line["extra"] = extras(dev)
         if world == 1 and not args.no_cpu:
             v, threads, sample, _, _ = cpu_baseline(args.config)
             line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads,
                                     "kind": "reference", "sample": sample,
                                     "value_1_thread": cpu_single_thread(args.config),
                                     "cpu": cpu_model()}
+            line["parity_vs_dll"] = dict(errors_vs_dll(args.config, dev), sample=sample)
+        if world == 1 and not args.no_extras and args.config == "cylinder2d":
+            line["extra"] = extras(dev, with_dll=not args.no_cpu, tile=tile or None)
         print(json.dumps(line), flush=True)
     return line
 
@@ -502,11 +589,17 @@ def time_launches(kernel, variant, dd, dv, n_mesh, reps):
     return start.elapsed_time(stop)*1e-3/reps
 
 
-def single_config(name, qv, pars, dtype, reps, dev):
-    """evals/s of one plain call shape (inputs resident)."""
-    from sasmodels_b200 import load_model
+def single_config(name, qv, pars, dtype, reps, dev, form=None, tile=None):
+    """evals/s of one plain call shape (inputs resident); `form` "plugin"
+    runs the plugin's C as translated where the model has a hoisted
+    binding; `tile` fixes the tile code."""
+    from sasmodels_b200 import _abi, load_model
     model = load_model(name, dtype=dtype, device=dev)
+    if form is not None:
+        model.lib = _abi.load_library(name, form=form)
     kernel = model.make_kernel(qv)
+    if tile is not None:
+        kernel.tile = tile
     details, values, magnetic = marshal(model.info, pars, qv)
     dd, dv = kernel.upload(details, values)
     t = time_launches(kernel, kernel.variant(magnetic), dd, dv, details.num_eval, reps)
@@ -658,44 +751,98 @@ def smear_compare(dev, reps=50):
     return out
 
 
-def f32c_error(name, qv, pars, dev):
-    """Max relative difference of the FP32c I(q) from the FP64 I(q)."""
-    from sasmodels_b200 import load_model
-    from sasmodels_b200.direct_model import call_kernel
-    out = []
-    for dtype in ("double", "float32c"):
-        kernel = load_model(name, dtype=dtype, device=dev).make_kernel(qv)
-        out.append(call_kernel(kernel, dict(pars)))
-        kernel.release()
-    return float(np.max(np.abs(out[1] - out[0])/np.abs(out[0])))
-
-
-def extras(dev):
-    """Secondary measurements of the other headline configurations."""
+def extras(dev, with_dll=True, tile=None):
+    """Secondary measurements of the other headline configurations; with
+    `with_dll`, each FP64 and FP32c form's max relative error against the
+    reference DLL on that configuration's bounded CPU sample."""
     from sasmodels_b200 import workloads
     out = {}
     name, qv, pars = workloads.sphere_1d()
-    v, t = single_config(name, qv, pars, "double", 200, dev)
-    out["sphere1d_f64"] = {"evals_per_s": v, "ms_per_call": 1e3*t}
+    for dtype in ("double", "float32c"):
+        v, t = single_config(name, qv, pars, dtype, 200, dev)
+        out["sphere1d_" + dtype] = {"evals_per_s": v, "ms_per_call": 1e3*t}
     name, qv, pars = workloads.cylinder_2d()
     v, t = single_config(name, qv, pars, "float32c", 3, dev)
-    out["cylinder2d_float32c"] = {"evals_per_s": v, "ms_per_call": 1e3*t,
-                                  "max_rel_err_vs_f64": f32c_error(name, qv, pars, dev)}
+    out["cylinder2d_float32c"] = {"evals_per_s": v, "ms_per_call": 1e3*t}
+    v, t = single_config(name, qv, pars, "double", 3, dev, form="plugin", tile=tile)
+    out["cylinder2d_plugin_f64"] = {
+        "evals_per_s": v, "ms_per_call": 1e3*t, "tile": "0x%08x" % tile if tile else None,
+        "what": "the plugin's Iqac as translated, without the hoisted binding, on the "
+                "headline's tile"}
     name, qv, pars = workloads.core_shell_sphere_magnetic()
     for dtype in ("double", "float32c"):
         v, t = single_config(name, qv, pars, dtype, 20, dev)
         out["magnetic_" + dtype] = {"evals_per_s": v, "ms_per_call": 1e3*t,
                                     "spin_channels": 6}
+    if with_dll:
+        for config, keys in (("sphere1d", ("sphere1d_double", "sphere1d_float32c")),
+                             ("cylinder2d", (None, "cylinder2d_float32c")),
+                             ("magnetic", ("magnetic_double", "magnetic_float32c"))):
+            errs = errors_vs_dll(config, dev)
+            for key, tag in zip(keys, ("f64", "f32c")):
+                if key is not None:
+                    out[key]["max_rel_err_vs_dll"] = errs["max_rel_err_vs_dll_" + tag]
+                    out[key]["dll_sample"] = sample_workload(config)[1]
     out["population"] = population_compare(4096, 7, dev)
+    if with_dll:
+        out["population"]["vs_dll"] = population_vs_dll(dev)
     out["smear_pinhole1d"] = smear_compare(dev)
     return out
 
 
-#: FP64 flops issued per evaluation of each workload's dominant kernel,
-#: from the ncu instruction counters of iq_main (2*DFMA + DADD + DMUL per
-#: thread instruction) divided by the evaluations of the captured launch
-#: (profiles/iq_main_cylinder2d.md, profiles/iq_main_magnetic.md).
-FLOPS_PER_EVAL = {"cylinder2d": 160.8, "magnetic": 758.0}
+def population_vs_dll(dev, stride=97, nq_sub=8, max_mesh=60000):
+    """Batched FP32c and FP64 I(q) against the reference DLL on every
+    `stride`-th set of the seeded population with a dispersity mesh of at
+    most `max_mesh` points, each at `nq_sub` of its q points (smallest and
+    largest kept), the DLL sharded over host threads by mesh range."""
+    from oracle import refdll
+    from sasmodels_b200 import load_model_info, workloads
+    from sasmodels_b200.batch import Population
+    pop = workloads.population(n_sets=4096, seed=1)[::stride]
+    by = {}
+    for name, q, pars in pop:
+        idx = np.unique(np.linspace(0, len(q) - 1, nq_sub).round().astype(int))
+        info = load_model_info(name)
+        details, values, _ = marshal(info, pars, [q[idx]])
+        if details.num_eval > max_mesh:
+            continue
+        by.setdefault(name, []).append((q[idx], pars, details, values))
+    out = {"sets": sum(len(v) for v in by.values()),
+           "sample": "every %d-th of 4096 seeded sets with <= %d mesh points, %d q each"
+                     % (stride, max_mesh, nq_sub)}
+    threads = host_threads()
+    for form in ("double", "float32c"):
+        worst = 0.0
+        for name, members in by.items():
+            P = Population(name, [(q, p) for q, p, _, _ in members], form=form, device=dev)
+            P.run()
+            for (q, _, details, values), iq in zip(members, P.iq()):
+                raw = refdll.run_mesh_threads(name, "Iq", q, details.buffer, values, 2,
+                                              threads)
+                ref = normalised_iq(raw, 2, len(q), values)
+                worst = max(worst, float(np.max(np.abs(iq - ref)/np.abs(ref))))
+        out["max_rel_err_vs_dll_" + ("f64" if form == "double" else "f32c")] = worst
+    return out
+
+
+#: Algorithmic work of each configuration per step, in SAS-flops (the
+#: "SAS-flop v1" convention: +,-,*,compare 1; / and sqrt 4; sin, cos, exp,
+#: log 16; sincos 24): the reference's own model C run on the
+#: configuration's inputs with a counting arithmetic type, every branch
+#: replayed, split into per-evaluation, per-mesh-point and per-q work.
+#: Produced by `python oracle/build_oracle.py && python oracle/sasflops.py
+#: sphere1d magnetic cylinder2d` (profiles/sasflops_counts.md).
+SASFLOPS = {
+    "cylinder2d": {"evals": 32112640000, "eval": 3316854138640, "point": 73500000, "q": 0},
+    "sphere1d": {"evals": 35000, "eval": 1672720, "point": 350, "q": 0},
+    "magnetic": {"evals": 17547264, "eval": 11053000224, "point": 12852, "q": 13074432},
+}
+#: FP64 flops issued per evaluation by the current iq_main of each
+#: configuration, from ncu's instruction counters (2 x DFMA + DMUL + DADD
+#: per thread instruction) over the evaluations of the captured launch; the
+#: issued count includes the operations CUDA's sin, sqrt and division expand
+#: into, so it sits above the algorithmic count (profiles/iq_main_*.md).
+ISSUED_FP64_PER_EVAL = {"magnetic": 758.0}
 #: XU-pipe (MUFU sin/cos/rcp/rsqrt and conversions) thread operations per
 #: evaluation of the FP32c form of iq_main: ncu's sm__inst_executed_pipe_xu
 #: (51.6 % of a 16-lane-per-clock peak over the elapsed cycles) x 32 lanes
@@ -724,6 +871,72 @@ def run_population(args, world, rank, local):
                                         "sample": rep["sample"]},
         "population": rep,
     }
+    print(json.dumps(line), flush=True)
+
+
+def run_population_split(args, world, rank, local):
+    """The fit-population sample (every `--pop-stride`-th of the 4096 seeded
+    sets) split over the ranks by estimated cost (multigpu.shard_by_cost,
+    per model); each rank evaluates its share as one batched FP32c launch
+    per model and the I(q) of all sets are all-gathered as device tensors
+    inside each step.  Total work is fixed as N grows ("strong")."""
+    import torch
+    from sasmodels_b200 import multigpu, workloads
+    from sasmodels_b200.batch import Population
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    pop = workloads.population(n_sets=4096, seed=1)[::args.pop_stride]
+    pops = []
+    for name in workloads.POP_MODELS:
+        sets = [(q, p) for n, q, p in pop if n == name]
+        parts = multigpu.shard_by_cost(multigpu.population_cost(name, sets), world)
+        mine = [sets[i] for i in parts[rank]]
+        if mine:
+            pops.append(Population(name, mine, form="float32c", device=dev))
+    cur = torch.cuda.current_stream()
+
+    def step():
+        for P in pops:
+            P.stream.wait_stream(cur)
+            P.run()
+            cur.wait_stream(P.stream)
+        flat = (torch.cat([P.d_iq for P in pops]) if pops else
+                torch.zeros(0, dtype=torch.float64, device=dev))
+        return multigpu.gather_blocks(flat)
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    times = []
+    with ClockSampler(local) as clocks:
+        barrier()
+        for _ in range(args.steps):
+            start = torch.cuda.Event(enable_timing=True)
+            stop = torch.cuda.Event(enable_timing=True)
+            start.record(cur)
+            step()
+            stop.record(cur)
+            times.append((start, stop))
+        barrier()
+    t_total = dist_max(sum(a.elapsed_time(b)*1e-3 for a, b in times))
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": len(pop)*args.steps/t_total, "unit": "param-sets/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3*t_total/args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32 compensated (f64 phases and sums)", "data": "synthetic",
+        "config": {"workload": "ellipsoid + core_shell_cylinder 1D population",
+                   "sample": "every %d-th of 4096 seeded sets (%d sets)"
+                             % (args.pop_stride, len(pop)),
+                   "parallelism": "population split by cost x%d, I(q) all-gathered as "
+                                  "device tensors inside each step" % world},
+        "gpu_launches": 3*len(workloads.POP_MODELS)*args.steps,
+    }
+    summary = clocks.summary()
+    if summary:
+        line["clocks"] = summary
     print(json.dumps(line), flush=True)
 
 
@@ -775,6 +988,10 @@ def main(argv=None):
                     help="q grid edge for cylinder2d (smaller for profiling)")
     ap.add_argument("--dtype", default="double", choices=["double", "float32c"],
                     help="arithmetic of the timed kernel (cylinder2d, magnetic, sphere1d)")
+    ap.add_argument("--split", default="q", choices=["q", "replicas"],
+                    help="N > 1: split one image into contiguous q blocks (default), or "
+                         "run one whole workload per GPU; --config population always "
+                         "splits the sets by cost")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
@@ -788,7 +1005,10 @@ def main(argv=None):
         elif args.config == "surrogate":
             run_surrogate(args, world, rank, local)
         elif args.config == "population":
-            run_population(args, world, rank, local)
+            if world > 1:
+                run_population_split(args, world, rank, local)
+            else:
+                run_population(args, world, rank, local)
         else:
             run_b200(args, world, rank, local)
     finally:

@@ -40,7 +40,11 @@
  * All arrays are DEVICE pointers (any allocator).  Added arguments:
  *   workspace, workspace_bytes  device scratch; sasb200_<model>_workspace_bytes
  *                 gives the size for a whole mesh in one pass; a smaller
- *                 workspace is used by processing the mesh in chunks
+ *                 workspace is used by processing the mesh in chunks.  A
+ *                 mesh range small enough for the single-launch path (its
+ *                 table fits 32 KB of one block's shared memory: 1024 points
+ *                 for sphere, 512 for cylinder 1D) uses no workspace, and
+ *                 workspace may then be NULL
  *   tile          iq_main tile code (splits<<16 | warps<<8 | lanes_per_q),
  *                 0 = built-in choice; see sasb200_<model>_tile_code
  *   stream        cudaStream_t (NULL = legacy default stream)
@@ -75,6 +79,11 @@ extern "C" {
     /* number of instantiated tile shapes and the code of shape i (autotuner) */ \
     int32_t sasb200_##M##_tile_count(void); \
     int32_t sasb200_##M##_tile_code(int32_t i); \
+    /* largest mesh range (pd_stop - pd_start) evaluated by the single-launch \
+     * path (one kernel, no workspace) for variant 0=Iq 1=Iqxy 2=Imagnetic; \
+     * larger ranges take three launches per workspace chunk; no reference \
+     * counterpart */ \
+    int32_t sasb200_##M##_single_launch_max(int32_t variant); \
     /* tile code the library picks for (nq, n_mesh) when tile == 0 */ \
     int32_t sasb200_##M##_default_tile(int32_t nq, int32_t n_mesh); \
     /* message of the last failed call on this host thread ("" if none) */ \
@@ -82,6 +91,17 @@ extern "C" {
 
 SASB200_DECLARE_MODEL(sphere)
 SASB200_DECLARE_MODEL(cylinder)
+
+/*
+ * The cylinder library's sasb200_cylinder_Iqxy runs a hand-rearranged FP64
+ * form of the plugin's Iqac (cylinder.c:92-102, lib/sas_J1.c:107-153) with
+ * the per-mesh-point work (contrast x volume, scale factor, weight, R, L/2,
+ * rotation row) hoisted out of the q loop and fewer divisions in J1; within
+ * 1e-12 of the reference DLL like every FP64 entry point.  The plugin's C as
+ * translated, without that rearrangement, stays exported under the prefix
+ * cylinder_plugin (same arguments) for comparison.
+ */
+SASB200_DECLARE_MODEL(cylinder_plugin)
 
 /*
  * Allocation-free variant of sasb200_cylinder_Iqxy.  No counterpart in the

@@ -73,6 +73,7 @@ class ModelLib:
         self._tile = self._fn("tile_code", ct.c_int32, [ct.c_int32])
         self._default_tile = self._fn("default_tile", ct.c_int32,
                                       [ct.c_int32, ct.c_int32])
+        self._single_max = self._fn("single_launch_max", ct.c_int32, [ct.c_int32])
 
     def _fn(self, suffix, restype, argtypes):
         fn = getattr(self.lib, "sasb200_%s_%s" % (self.name, suffix))
@@ -93,6 +94,20 @@ class ModelLib:
     def default_tile(self, nq, n_mesh):
         return int(self._default_tile(nq, n_mesh))
 
+    def single_launch_max(self, variant):
+        """Largest mesh range the library evaluates in one kernel launch."""
+        return int(self._single_max(VARIANT_ID[variant]))
+
+    def launches(self, variant, nq, n_mesh, workspace_bytes=None, tile=0):
+        """Kernel launches of one call over a mesh range of n_mesh points
+        (1 on the single-launch path, else 3 per workspace chunk)."""
+        if n_mesh <= self.single_launch_max(variant):
+            return 1
+        full = self.workspace_bytes(variant, nq, n_mesh, tile)
+        if workspace_bytes is None or workspace_bytes >= full:
+            return 3*max(1, -(-n_mesh//(1 << 20)))
+        return 3*max(1, -(-full//max(workspace_bytes, 1)))
+
     def call(self, variant, nq, pd_start, pd_stop, details, values, q, result,
              cutoff, reff_mode, workspace, workspace_bytes, tile, stream):
         status = self.kernels[variant](
@@ -103,12 +118,20 @@ class ModelLib:
                 self.name, variant, status, self.last_error()))
 
 
+#: symbol prefix of each form within a model's library: the FP64 form, the
+#: FP32-compensated form, and (for models with a hoisted FP64 binding) the
+#: plugin's C as translated, without the hoisting
+FORM_PREFIX = {"double": "%s", "float32c": "%s_f32c", "plugin": "%s_plugin"}
+
+
 def load_library(name, lib_dir=None, form="double"):
-    """Entry points of model *name*; *form* is "double" or "float32c"."""
+    """Entry points of model *name*; *form* is "double", "float32c" or
+    "plugin"."""
     key = (name, lib_dir, form)
     if key not in _LOADED:
-        prefix = name if form == "double" else name + "_f32c"
-        _LOADED[key] = ModelLib(prefix, library_path(name, lib_dir))
+        if form not in FORM_PREFIX:
+            raise ValueError("unknown form %r" % (form,))
+        _LOADED[key] = ModelLib(FORM_PREFIX[form] % name, library_path(name, lib_dir))
     return _LOADED[key]
 
 

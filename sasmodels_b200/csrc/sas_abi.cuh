@@ -5,6 +5,7 @@
 //   int32_t  sasb200_<name>_Iq(...), _Iqxy(...), _Imagnetic(...)
 //   uint64_t sasb200_<name>_workspace_bytes(variant, nq, n_mesh, tile)
 //   int32_t  sasb200_<name>_tile_count(void), sasb200_<name>_tile_code(i)
+//   int32_t  sasb200_<name>_single_launch_max(variant)
 //   const char *sasb200_<name>_last_error(void)
 //
 // The three kernels take the arguments of the reference DLL symbols
@@ -149,6 +150,27 @@ __host__ bool dispatch_main(Tile t, dim3 grid, cudaStream_t st, int nq, const do
     }
 }
 
+template <class M, int VAR>
+__host__ bool dispatch_small(Tile t, int nq, cudaStream_t st, int pd_start, int n_mesh,
+                             const int32_t *details, const double *values, const double *q,
+                             double cutoff, int reff_mode, double *result, int accumulate)
+{
+    const dim3 grid(nq > 0 ? (nq + t.lq - 1)/t.lq : 1);
+#define SASB200_SMALL(LQ_, W_) \
+    iq_small<M, VAR, LQ_, W_><<<grid, 32*(W_), 0, st>>>(nq, pd_start, n_mesh, details, \
+        values, q, cutoff, reff_mode, result, accumulate); return true;
+    switch (t.lq*100 + t.warps) {
+    case 3204: SASB200_SMALL(32, 4)
+    case 3208: SASB200_SMALL(32, 8)
+    case 804:  SASB200_SMALL(8, 4)
+    case 808:  SASB200_SMALL(8, 8)
+    case 104:  SASB200_SMALL(1, 4)
+    case 108:  SASB200_SMALL(1, 8)
+    default: return false;
+    }
+#undef SASB200_SMALL
+}
+
 // Error text of the last failing call on this host thread.
 inline char *error_buffer()
 {
@@ -195,6 +217,20 @@ __host__ int32_t run(int32_t nq, int32_t pd_start, int32_t pd_stop,
     Tile t = tile_code ? tile_decode(tile_code) : choose_tile(nq, n_mesh);
     if (!shape_ok(t) || t.splits < 1)
         return fail(ERR_ARGUMENT, "unknown tile code");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (n_mesh <= small_mesh_max<M, VAR>()) {
+        // the whole mesh range fits one block's shared memory: one launch,
+        // no workspace (mesh splits of the tile code do not apply)
+        if (!dispatch_small<M, VAR>(t, nq, st, pd_start, n_mesh, details, values, q,
+                                    cutoff, reff_mode, result, pd_start > 0 ? 1 : 0))
+            return fail(ERR_ARGUMENT, "unknown tile shape");
+        const cudaError_t err = cudaGetLastError();
+        if (err != cudaSuccess) {
+            std::snprintf(error_buffer(), 256, "kernel launch: %s", cudaGetErrorString(err));
+            return ERR_CUDA;
+        }
+        return OK;
+    }
     // largest chunk of whole segments whose workspace fits
     const long long nseg_all = n_mesh > 0 ? (n_mesh + SEG - 1)/SEG : 1;
     long long lo = 0, hi = nseg_all;
@@ -217,7 +253,6 @@ __host__ int32_t run(int32_t nq, int32_t pd_start, int32_t pd_stop,
     // the norms in the DLL's own order when an effective radius is asked for
     double *seq = reff_mode != 0 ? points : nullptr;
     const int points_stride = (int)(((chunk + SEG - 1)/SEG)*SEG);
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int nout_nq = L::NOUT*nq;
 
     long long start = pd_start;
@@ -295,6 +330,15 @@ extern "C" uint64_t sasb200_##NAME##_workspace_bytes(                           
     case 1: return sasb200::workspace_bytes<MODEL, sasb200::VAR_IQXY>(nq, n_mesh, tile);\
     case 2: return sasb200::workspace_bytes<MODEL, sasb200::VAR_IMAGNETIC>(nq, n_mesh,  \
                                                                            tile);       \
+    default: return 0;                                                                  \
+    }                                                                                   \
+}                                                                                       \
+extern "C" int32_t sasb200_##NAME##_single_launch_max(int32_t variant)                  \
+{                                                                                       \
+    switch (variant) {                                                                  \
+    case 0: return sasb200::small_mesh_max<MODEL, sasb200::VAR_IQ>();                   \
+    case 1: return sasb200::small_mesh_max<MODEL, sasb200::VAR_IQXY>();                 \
+    case 2: return sasb200::small_mesh_max<MODEL, sasb200::VAR_IMAGNETIC>();            \
     default: return 0;                                                                  \
     }                                                                                   \
 }                                                                                       \

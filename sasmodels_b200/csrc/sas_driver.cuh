@@ -57,15 +57,55 @@ struct DetailsView {
     __device__ int theta_par() const { return buf[4*MPD + 3]; }
 };
 
+// A binding may restate one 2D form of its model with the per-mesh-point
+// invariants hoisted out of the q loop: it declares `HOIST` (the XY mode it
+// covers), `NH` (doubles per table row), `hoist_row(weight, v, rot, row)`
+// (run once per kept mesh point by mesh_prepare) and
+// `eval_row(qx, qy, qsq, row)` (returns weight * F^2 for one q).  Bindings
+// without these keep the generic [weight, v, rotation] rows.
+template <class M, class = void>
+struct hoist_mode { static constexpr int value = 0; };
+template <class M>
+struct hoist_mode<M, decltype((void)M::HOIST, void())> {
+    static constexpr int value = M::HOIST;
+};
+template <class M, class = void>
+struct hoist_width { static constexpr int value = 1; };
+template <class M>
+struct hoist_width<M, decltype((void)M::NH, void())> {
+    static constexpr int value = M::NH;
+};
+
 // Per-variant table layout.
 template <class M, int VAR>
 struct Layout {
     static constexpr int XY = (VAR == VAR_IQ) ? XY_1D : M::XY_MODE;
     static constexpr int NROT = (XY == XY_QAC) ? 2 : (XY == XY_QABC) ? 6 : 0;
     static constexpr int NP = M::NPARS > 0 ? M::NPARS : 1;
-    static constexpr int NF = ((1 + M::NPARS + NROT) + 1) & ~1;   // 16-byte rows
+    static constexpr bool HOISTED = (VAR == VAR_IQXY) && hoist_mode<M>::value == XY
+                                    && XY != XY_1D;
+    static constexpr int NF = HOISTED ? ((hoist_width<M>::value + 1) & ~1)
+                                      : ((1 + M::NPARS + NROT) + 1) & ~1;  // 16-byte rows
     static constexpr bool FQ1D = (VAR == VAR_IQ) && M::HAVE_FQ;
     static constexpr int NOUT = FQ1D ? 2 : 1;
+};
+
+// Hoisted-row hooks, reached only when Layout<M, VAR>::HOISTED.
+template <class M, bool ON>
+struct HoistOps {
+    __device__ static void row(double, const double *, const double *, double *) {}
+    __device__ static double eval(double, double, double, const double *) { return 0.0; }
+};
+template <class M>
+struct HoistOps<M, true> {
+    __device__ static void row(double w, const double *v, const double *rot, double *r)
+    {
+        M::hoist_row(w, v, rot, r);
+    }
+    __device__ static double eval(double qx, double qy, double qsq, const double *r)
+    {
+        return M::eval_row(qx, qy, qsq, r);
+    }
 };
 
 // ------------------------------------------------------------- rotations ---
@@ -207,6 +247,93 @@ __device__ __forceinline__ double eval_2d(double qx, double qy, double qk,
     }
 }
 
+// ------------------------------------------------------ one mesh point ---
+
+// Decode mesh point `step` (mixed radix over the pd dimensions, weight
+// product outermost first, kernel_iq.c:642-664), apply VALID, the jitter
+// projection (kernel_iq.c:621-626) and the cutoff, and for a kept point its
+// volumes, effective radius and rotation (kernel_iq.c:720-734, 197-312).
+// Returns whether the point is kept.
+template <class M, int VAR>
+__device__ __forceinline__ bool decode_point(
+    int step, const DetailsView<M::MAX_PD> &det, const double *__restrict__ values,
+    double cutoff, int reff_mode, double *v, double &weight, double &form,
+    double &shell, double &reff, double *rot)
+{
+    using L = Layout<M, VAR>;
+    constexpr int MPD = M::MAX_PD;
+    #pragma unroll
+    for (int k = 0; k < M::NPARS; ++k) v[k] = values[2 + k];
+    // Oriented 2D kernels start from zero jitter (kernel_iq.c:614-616, 559).
+    if constexpr (L::XY == XY_QAC || L::XY == XY_QABC) {
+        if (M::THETA_PAR >= 0) {
+            v[M::THETA_PAR] = 0.0;
+            v[M::THETA_PAR + 1] = 0.0;
+            if (L::XY == XY_QABC) v[M::THETA_PAR + 2] = 0.0;
+        }
+    }
+    const double *pd_value = values + M::NVALUES;
+    const double *pd_weight = pd_value + det.num_weights();
+    double w = 1.0;
+    #pragma unroll
+    for (int d = MPD - 1; d >= 0; --d) {
+        // lengths and strides were validated on the host; the max() only
+        // keeps a malformed buffer from dividing by zero
+        const int n = max(det.pd_length(d), 1);
+        const int i = (step/max(det.pd_stride(d), 1)) % n;
+        const int off = det.pd_offset(d) + i;
+        const int p = det.pd_par(d);
+        const double pv = pd_value[off];
+        #pragma unroll
+        for (int k = 0; k < M::NPARS; ++k) if (k == p) v[k] = pv;
+        w = pd_weight[off]*w;
+    }
+    if (!M::valid(v)) return false;
+    if constexpr (L::XY == XY_QAC || L::XY == XY_QABC) {
+        const double dtheta = v[M::THETA_PAR];
+        weight = fabs(cos(dtheta*M_PI_180))*w;     // equirectangular
+    } else {
+        weight = w;
+    }
+    if constexpr (L::XY == XY_QXY) {
+        // models taking the angles directly see the view angles
+        if (M::HAVE_THETA) {
+            v[M::THETA_PAR] = values[M::THETA_PAR + 2];
+            v[M::THETA_PAR + 1] = values[M::THETA_PAR + 3];
+            if (M::HAVE_PSI) v[M::THETA_PAR + 2] = values[M::THETA_PAR + 4];
+        }
+    }
+    if (!(weight > cutoff)) return false;
+    M::volume(v, form, shell);
+    if (reff_mode != 0) reff = M::reff(reff_mode, v);
+    if constexpr (L::XY == XY_QAC) {
+        rotation_ac(values[M::THETA_PAR + 2], values[M::THETA_PAR + 3],
+                    v[M::THETA_PAR], v[M::THETA_PAR + 1], rot);
+    } else if constexpr (L::XY == XY_QABC) {
+        rotation_abc(values[M::THETA_PAR + 2], values[M::THETA_PAR + 3],
+                     values[M::THETA_PAR + 4], v[M::THETA_PAR],
+                     v[M::THETA_PAR + 1], v[M::THETA_PAR + 2], rot);
+    }
+    return true;
+}
+
+// One table row: [weight, p[0..NPARS), rotation] or the binding's hoisted row.
+template <class M, int VAR>
+__device__ __forceinline__ void write_row(double *row, double weight, const double *v,
+                                          const double *rot)
+{
+    using L = Layout<M, VAR>;
+    if constexpr (L::HOISTED) {
+        HoistOps<M, true>::row(weight, v, rot, row);
+    } else {
+        row[0] = weight;
+        #pragma unroll
+        for (int k = 0; k < M::NPARS; ++k) row[1 + k] = v[k];
+        #pragma unroll
+        for (int r = 0; r < L::NROT; ++r) row[1 + M::NPARS + r] = rot[r];
+    }
+}
+
 // ----------------------------------------------------------- mesh_prepare ---
 
 template <class M, int VAR>
@@ -217,9 +344,8 @@ mesh_prepare(int pd_start, int n_mesh, const int32_t *__restrict__ details,
              double *__restrict__ seg_norm, double *__restrict__ points, int points_stride)
 {
     using L = Layout<M, VAR>;
-    constexpr int MPD = M::MAX_PD;
     constexpr int NF = L::NF;
-    const DetailsView<MPD> det{details};
+    const DetailsView<M::MAX_PD> det{details};
     const int t = threadIdx.x;
     const int local = blockIdx.x*SEG + t;
     const int step = pd_start + local;
@@ -230,63 +356,8 @@ mesh_prepare(int pd_start, int n_mesh, const int32_t *__restrict__ details,
     double rot[L::NROT > 0 ? L::NROT : 1];
 
     if (local < n_mesh) {
-        #pragma unroll
-        for (int k = 0; k < M::NPARS; ++k) v[k] = values[2 + k];
-        // Oriented 2D kernels start from zero jitter (kernel_iq.c:614-616, 559).
-        if constexpr (L::XY == XY_QAC || L::XY == XY_QABC) {
-            if (M::THETA_PAR >= 0) {
-                v[M::THETA_PAR] = 0.0;
-                v[M::THETA_PAR + 1] = 0.0;
-                if (L::XY == XY_QABC) v[M::THETA_PAR + 2] = 0.0;
-            }
-        }
-        const double *pd_value = values + M::NVALUES;
-        const double *pd_weight = pd_value + det.num_weights();
-        // weight_d = w_d[i_d] * weight_{d+1}, outermost level first
-        // (kernel_iq.c:642-664)
-        double w = 1.0;
-        #pragma unroll
-        for (int d = MPD - 1; d >= 0; --d) {
-            // lengths and strides were validated on the host; the max() only
-            // keeps a malformed buffer from dividing by zero
-            const int n = max(det.pd_length(d), 1);
-            const int i = (step/max(det.pd_stride(d), 1)) % n;
-            const int off = det.pd_offset(d) + i;
-            const int p = det.pd_par(d);
-            const double pv = pd_value[off];
-            #pragma unroll
-            for (int k = 0; k < M::NPARS; ++k) if (k == p) v[k] = pv;
-            w = pd_weight[off]*w;
-        }
-        if (M::valid(v)) {
-            if constexpr (L::XY == XY_QAC || L::XY == XY_QABC) {
-                const double dtheta = v[M::THETA_PAR];
-                weight = fabs(cos(dtheta*M_PI_180))*w;     // equirectangular
-            } else {
-                weight = w;
-            }
-            if constexpr (L::XY == XY_QXY) {
-                // models taking the angles directly see the view angles
-                if (M::HAVE_THETA) {
-                    v[M::THETA_PAR] = values[M::THETA_PAR + 2];
-                    v[M::THETA_PAR + 1] = values[M::THETA_PAR + 3];
-                    if (M::HAVE_PSI) v[M::THETA_PAR + 2] = values[M::THETA_PAR + 4];
-                }
-            }
-            if (weight > cutoff) {
-                keep = true;
-                M::volume(v, form, shell);
-                if (reff_mode != 0) reff = M::reff(reff_mode, v);
-                if constexpr (L::XY == XY_QAC) {
-                    rotation_ac(values[M::THETA_PAR + 2], values[M::THETA_PAR + 3],
-                                v[M::THETA_PAR], v[M::THETA_PAR + 1], rot);
-                } else if constexpr (L::XY == XY_QABC) {
-                    rotation_abc(values[M::THETA_PAR + 2], values[M::THETA_PAR + 3],
-                                 values[M::THETA_PAR + 4], v[M::THETA_PAR],
-                                 v[M::THETA_PAR + 1], v[M::THETA_PAR + 2], rot);
-                }
-            }
-        }
+        keep = decode_point<M, VAR>(step, det, values, cutoff, reff_mode, v, weight, form,
+                                    shell, reff, rot);
     }
 
     // Block-local stable compaction: ballot within warps, prefix over warps.
@@ -315,12 +386,7 @@ mesh_prepare(int pd_start, int n_mesh, const int32_t *__restrict__ details,
     }
     if (keep) {
         const int pos = base + __popc(ballot & ((1u << lane) - 1u));
-        double *row = table + ((size_t)blockIdx.x*SEG + pos)*NF;
-        row[0] = weight;
-        #pragma unroll
-        for (int k = 0; k < M::NPARS; ++k) row[1 + k] = v[k];
-        #pragma unroll
-        for (int r = 0; r < L::NROT; ++r) row[1 + M::NPARS + r] = rot[r];
+        write_row<M, VAR>(table + ((size_t)blockIdx.x*SEG + pos)*NF, weight, v, rot);
     }
     // fixed-order tree for the four norm sums
     #pragma unroll
@@ -340,6 +406,141 @@ mesh_prepare(int pd_start, int n_mesh, const int32_t *__restrict__ details,
 
 // ---------------------------------------------------------------- iq_main ---
 
+// Per-lane q point and what depends only on it: |q|, |q|^2 and, for the
+// magnetic variant, the effective slds of the five distinct spin channels
+// (kernel_iq.c:750-779, hoisted out of the mesh loop).
+template <class M, int VAR>
+struct QState {
+    using L = Layout<M, VAR>;
+    static constexpr bool MAG = (VAR == VAR_IMAGNETIC) && (M::NMAG > 0);
+    static constexpr int NMAGS = M::NMAG > 0 ? M::NMAG : 1;
+    double qk = 0.0, qx = 0.0, qy = 0.0, qsq = 0.0;
+    double eff[5][NMAGS];
+    double chan_w[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    bool mag_on = false;
+
+    // q is read only for a lane whose q_index is in range (ok): a call with
+    // no q points may pass no q array at all
+    __device__ __forceinline__ QState(const double *__restrict__ q, int q_index, bool ok,
+                                      const double *__restrict__ values)
+    {
+        if constexpr (L::XY == XY_1D) {
+            qk = ok ? q[q_index] : 0.0;
+        } else {
+            qx = ok ? q[2*q_index] : 0.0;
+            qy = ok ? q[2*q_index + 1] : 0.0;
+            qsq = qx*qx + qy*qy;
+            if constexpr (!L::HOISTED) qk = sqrt(qsq);
+        }
+        if constexpr (MAG) {
+            SpinSetup s;
+            spin_setup(values, M::NPARS, s);
+            mag_on = (qx*qx + qy*qy) > 1.e-16;
+            // channels whose weight is significant (kernel_iq.c:759-761); the
+            // two real spin-flip channels see identical slds and share one
+            // evaluation
+            chan_w[0] = s.w[0] > 1.e-8 ? s.w[0] : 0.0;
+            chan_w[1] = (s.w[1] > 1.e-8 ? s.w[1] : 0.0) + (s.w[2] > 1.e-8 ? s.w[2] : 0.0);
+            chan_w[2] = s.w[3] > 1.e-8 ? s.w[3] : 0.0;
+            chan_w[3] = s.w[4] > 1.e-8 ? s.w[4] : 0.0;
+            chan_w[4] = s.w[5] > 1.e-8 ? s.w[5] : 0.0;
+            #pragma unroll
+            for (int sk = 0; sk < M::NMAG; ++sk) {
+                const int idx = M::mag_par(sk);
+                const double *m = values + M::NPARS + 6 + 3*sk;
+                double e5[5];
+                if (mag_on) magnetic_slds(s, qx, qy, values[idx + 2], m[0], m[1], m[2], e5);
+                else { e5[0] = e5[1] = e5[2] = e5[3] = e5[4] = 0.0; }
+                #pragma unroll
+                for (int c = 0; c < 5; ++c) eff[c][sk] = e5[c];
+            }
+        }
+    }
+};
+
+// Add w F^2 (and w F) of table rows j0, j0 + step, ... < cnt to acc2 (acc1).
+template <class M, int VAR>
+__device__ __forceinline__ void accumulate_rows(const QState<M, VAR> &qs,
+                                                const double *rows, int j0, int cnt,
+                                                int step, double &acc2, double &acc1)
+{
+    using L = Layout<M, VAR>;
+    constexpr int NF = L::NF;
+    constexpr int XY = L::XY;
+    if constexpr (L::HOISTED) {
+        for (int j = j0; j < cnt; j += step)
+            acc2 += HoistOps<M, true>::eval(qs.qx, qs.qy, qs.qsq, rows + j*NF);
+    } else {
+        for (int j = j0; j < cnt; j += step) {
+            const double *row = rows + j*NF;
+            const double w = row[0];
+            double v[L::NP];
+            #pragma unroll
+            for (int k = 0; k < M::NPARS; ++k) v[k] = row[1 + k];
+            const double *rot = row + 1 + M::NPARS;
+            if constexpr (XY == XY_1D) {
+                if constexpr (L::FQ1D) {
+                    double F1, F2;
+                    M::fq(qs.qk, F1, F2, v);
+                    acc2 += w*F2;
+                    acc1 += w*F1;
+                } else {
+                    acc2 += w*M::iq(qs.qk, v);
+                }
+            } else if constexpr (QState<M, VAR>::MAG) {
+                double F2 = 0.0;
+                if (qs.mag_on) {
+                    #pragma unroll
+                    for (int c = 0; c < 5; ++c) {
+                        if (qs.chan_w[c] > 0.0) {
+                            #pragma unroll
+                            for (int sk = 0; sk < M::NMAG; ++sk)
+                                v[M::mag_par(sk)] = qs.eff[c][sk];
+                            F2 += qs.chan_w[c]*eval_2d<M, XY>(qs.qx, qs.qy, qs.qk, rot, v);
+                        }
+                    }
+                }
+                acc2 += w*F2;
+            } else {
+                acc2 += w*eval_2d<M, XY>(qs.qx, qs.qy, qs.qk, rot, v);
+            }
+        }
+    }
+}
+
+// Reduce the per-lane sums of a block to one value per q: butterfly over the
+// mesh-lane bits of each warp, then across warps in warp order.  Returns the
+// sums in lanes with ml == 0 of warp 0.
+template <int LQ, int WARPS, int NOUT>
+__device__ __forceinline__ void reduce_block(double &acc2, double &acc1,
+                                             double (*red)[LQ][NOUT])
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int qi = lane % LQ;
+    const int ml = lane / LQ;
+    #pragma unroll
+    for (int off = LQ; off < 32; off <<= 1) {
+        acc2 += __shfl_xor_sync(FULL_MASK, acc2, off);
+        if constexpr (NOUT == 2) acc1 += __shfl_xor_sync(FULL_MASK, acc1, off);
+    }
+    if (ml == 0) {
+        red[warp][qi][0] = acc2;
+        if constexpr (NOUT == 2) red[warp][qi][1] = acc1;
+    }
+    __syncthreads();
+    if (warp == 0 && ml == 0) {
+        double s2 = 0.0, s1 = 0.0;
+        #pragma unroll
+        for (int k = 0; k < WARPS; ++k) {
+            s2 += red[k][qi][0];
+            if constexpr (NOUT == 2) s1 += red[k][qi][1];
+        }
+        acc2 = s2;
+        acc1 = s1;
+    }
+}
+
 template <class M, int VAR, int LQ, int WARPS>
 __global__ void __launch_bounds__(32*WARPS)
 iq_main(int nq, const double *__restrict__ q, const double *__restrict__ values,
@@ -349,9 +550,6 @@ iq_main(int nq, const double *__restrict__ q, const double *__restrict__ values,
     using L = Layout<M, VAR>;
     constexpr int NF = L::NF;
     constexpr int LM = 32/LQ;
-    constexpr int XY = L::XY;
-    constexpr bool MAG = (VAR == VAR_IMAGNETIC) && (M::NMAG > 0);
-    constexpr int NMAGS = M::NMAG > 0 ? M::NMAG : 1;
 
     extern __shared__ __align__(16) double stage[];     // SEG*NF doubles (dynamic)
     __shared__ double red[WARPS][LQ][L::NOUT];
@@ -362,43 +560,7 @@ iq_main(int nq, const double *__restrict__ q, const double *__restrict__ values,
     const int ml = lane / LQ;
     const int q_index = blockIdx.x*LQ + qi;
     const bool q_ok = q_index < nq;
-    const int qload = q_ok ? q_index : 0;
-
-    double qk = 0.0, qx = 0.0, qy = 0.0;
-    if constexpr (XY == XY_1D) {
-        qk = q[qload];
-    } else {
-        qx = q[2*qload];
-        qy = q[2*qload + 1];
-        qk = sqrt(qx*qx + qy*qy);
-    }
-
-    // magnetism: per-q effective slds, hoisted out of the mesh loop
-    double eff[5][NMAGS];
-    double chan_w[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    bool mag_on = false;
-    if constexpr (MAG) {
-        SpinSetup s;
-        spin_setup(values, M::NPARS, s);
-        mag_on = (qx*qx + qy*qy) > 1.e-16;
-        // channels whose weight is significant (kernel_iq.c:759-761); the two
-        // real spin-flip channels see identical slds and share one evaluation
-        chan_w[0] = s.w[0] > 1.e-8 ? s.w[0] : 0.0;
-        chan_w[1] = (s.w[1] > 1.e-8 ? s.w[1] : 0.0) + (s.w[2] > 1.e-8 ? s.w[2] : 0.0);
-        chan_w[2] = s.w[3] > 1.e-8 ? s.w[3] : 0.0;
-        chan_w[3] = s.w[4] > 1.e-8 ? s.w[4] : 0.0;
-        chan_w[4] = s.w[5] > 1.e-8 ? s.w[5] : 0.0;
-        #pragma unroll
-        for (int sk = 0; sk < M::NMAG; ++sk) {
-            const int idx = M::mag_par(sk);
-            const double *m = values + M::NPARS + 6 + 3*sk;
-            double e5[5];
-            if (mag_on) magnetic_slds(s, qx, qy, values[idx + 2], m[0], m[1], m[2], e5);
-            else { e5[0] = e5[1] = e5[2] = e5[3] = e5[4] = 0.0; }
-            #pragma unroll
-            for (int c = 0; c < 5; ++c) eff[c][sk] = e5[c];
-        }
-    }
+    const QState<M, VAR> qs(q, q_index, q_ok, values);
 
     const int s0 = (int)(((long long)blockIdx.y*nseg)/gridDim.y);
     const int s1 = (int)(((long long)(blockIdx.y + 1)*nseg)/gridDim.y);
@@ -410,65 +572,148 @@ iq_main(int nq, const double *__restrict__ q, const double *__restrict__ values,
         const double *src = table + (size_t)sgi*SEG*NF;
         for (int i = threadIdx.x; i < cnt*NF; i += 32*WARPS) stage[i] = src[i];
         __syncthreads();
-        for (int j = warp*LM + ml; j < cnt; j += WARPS*LM) {
-            const double *row = stage + j*NF;
-            const double w = row[0];
-            double v[L::NP];
+        accumulate_rows<M, VAR>(qs, stage, warp*LM + ml, cnt, WARPS*LM, acc2, acc1);
+    }
+
+    reduce_block<LQ, WARPS, L::NOUT>(acc2, acc1, red);
+    if (warp == 0 && ml == 0 && q_ok) {
+        double *out = partial + (size_t)blockIdx.y*L::NOUT*nq;
+        if constexpr (L::FQ1D) {
+            out[2*q_index] = acc2;
+            out[2*q_index + 1] = acc1;
+        } else {
+            out[q_index] = acc2;
+        }
+    }
+}
+
+// --------------------------------------------------------------- iq_small ---
+
+// Single-launch form for meshes whose table fits in shared memory
+// (n_mesh <= small_mesh_max<M, VAR>()): every block decodes the whole mesh
+// range into shared memory (stable compaction in mesh order), evaluates its q
+// tile over it and writes -- or, for a continued mesh (accumulate != 0), adds
+// to -- its q slots of result directly; block 0 also writes the four norm
+// sums.  There is no cross-block reduction, so one launch replaces
+// mesh_prepare + iq_main + finalize.  Norms: a fixed tree over the threads'
+// strided partial sums, or with an effective radius requested, one point at
+// a time in mesh order from the stored value (kernel_iq.c:720-734), as
+// finalize does.
+template <class M, int VAR>
+constexpr int small_mesh_max()
+{
+    // rows of the table within 32 KB of static shared memory (with the
+    // reduction buffers the block stays under the 48 KB static limit), whole
+    // warps
+    return ((32*1024/(Layout<M, VAR>::NF*8))/32)*32;
+}
+
+template <class M, int VAR, int LQ, int WARPS>
+__global__ void __launch_bounds__(32*WARPS)
+iq_small(int nq, int pd_start, int n_mesh, const int32_t *__restrict__ details,
+         const double *__restrict__ values, const double *__restrict__ q, double cutoff,
+         int reff_mode, double *__restrict__ result, int accumulate)
+{
+    using L = Layout<M, VAR>;
+    constexpr int NF = L::NF;
+    constexpr int LM = 32/LQ;
+    constexpr int T = 32*WARPS;
+    constexpr int CAP = small_mesh_max<M, VAR>();
+
+    __shared__ __align__(16) double rows[CAP*NF];
+    __shared__ double red[WARPS][LQ][L::NOUT];
+    __shared__ double nred[4][T];
+    __shared__ int warp_cnt[WARPS];
+
+    const DetailsView<M::MAX_PD> det{details};
+    const int t = threadIdx.x;
+    const int lane = t & 31;
+    const int warp = t >> 5;
+    const bool norms_here = blockIdx.x == 0;
+    const bool sequential = norms_here && reff_mode != 0;
+
+    // ---- the mesh range into shared memory, in mesh order ----
+    double nsum[4] = {0.0, 0.0, 0.0, 0.0};
+    double seq = 0.0;                        // thread k < 4: norm k in mesh order
+    if (sequential && t < 4) seq = accumulate ? result[L::NOUT*nq + t] : 0.0;
+    int base = 0;
+    for (int chunk = 0; chunk < n_mesh; chunk += T) {
+        const int local = chunk + t;
+        bool keep = false;
+        double v[L::NP];
+        double weight = 0.0, form = 0.0, shell = 0.0, reff = 0.0;
+        double rot[L::NROT > 0 ? L::NROT : 1];
+        if (local < n_mesh)
+            keep = decode_point<M, VAR>(pd_start + local, det, values, cutoff, reff_mode, v,
+                                        weight, form, shell, reff, rot);
+        const double term[4] = {keep ? weight : 0.0, keep ? weight*form : 0.0,
+                                keep ? weight*shell : 0.0, keep ? weight*reff : 0.0};
+        const unsigned ballot = __ballot_sync(FULL_MASK, keep);
+        if (lane == 0) warp_cnt[warp] = __popc(ballot);
+        if (sequential) {
             #pragma unroll
-            for (int k = 0; k < M::NPARS; ++k) v[k] = row[1 + k];
-            const double *rot = row + 1 + M::NPARS;
-            if constexpr (XY == XY_1D) {
-                if constexpr (L::FQ1D) {
-                    double F1, F2;
-                    M::fq(qk, F1, F2, v);
-                    acc2 += w*F2;
-                    acc1 += w*F1;
-                } else {
-                    acc2 += w*M::iq(qk, v);
-                }
-            } else if constexpr (MAG) {
-                double F2 = 0.0;
-                if (mag_on) {
+            for (int k = 0; k < 4; ++k) nred[k][t] = term[k];
+        } else {
+            #pragma unroll
+            for (int k = 0; k < 4; ++k) nsum[k] += term[k];
+        }
+        __syncthreads();
+        int before = 0, total = 0;
+        #pragma unroll
+        for (int k = 0; k < WARPS; ++k) {
+            if (k < warp) before += warp_cnt[k];
+            total += warp_cnt[k];
+        }
+        if (keep) {
+            const int pos = base + before + __popc(ballot & ((1u << lane) - 1u));
+            write_row<M, VAR>(rows + pos*NF, weight, v, rot);
+        }
+        if (sequential && t < 4) {
+            const int n = min(T, n_mesh - chunk);
+            for (int p = 0; p < n; ++p) seq = __dadd_rn(seq, nred[t][p]);
+        }
+        base += total;
+        __syncthreads();
+    }
+    const int cnt = base;
+
+    // ---- the norms (block 0) ----
+    if (norms_here) {
+        if (sequential) {
+            if (t < 4) result[L::NOUT*nq + t] = seq;
+        } else {
+            #pragma unroll
+            for (int k = 0; k < 4; ++k) nred[k][t] = nsum[k];
+            #pragma unroll
+            for (int s = T/2; s > 0; s >>= 1) {
+                __syncthreads();
+                if (t < s) {
                     #pragma unroll
-                    for (int c = 0; c < 5; ++c) {
-                        if (chan_w[c] > 0.0) {
-                            #pragma unroll
-                            for (int sk = 0; sk < M::NMAG; ++sk) v[M::mag_par(sk)] = eff[c][sk];
-                            F2 += chan_w[c]*eval_2d<M, XY>(qx, qy, qk, rot, v);
-                        }
-                    }
+                    for (int k = 0; k < 4; ++k) nred[k][t] += nred[k][t + s];
                 }
-                acc2 += w*F2;
-            } else {
-                acc2 += w*eval_2d<M, XY>(qx, qy, qk, rot, v);
+            }
+            if (t < 4) {
+                const double add = nred[t][0];
+                result[L::NOUT*nq + t] = accumulate ? result[L::NOUT*nq + t] + add : add;
             }
         }
     }
 
-    // lanes that share a q: butterfly over the mesh-lane bits
-    #pragma unroll
-    for (int off = LQ; off < 32; off <<= 1) {
-        acc2 += __shfl_xor_sync(FULL_MASK, acc2, off);
-        if constexpr (L::FQ1D) acc1 += __shfl_xor_sync(FULL_MASK, acc1, off);
-    }
-    if (ml == 0) {
-        red[warp][qi][0] = acc2;
-        if constexpr (L::FQ1D) red[warp][qi][1] = acc1;
-    }
-    __syncthreads();
+    // ---- this block's q tile over the table ----
+    const int qi = lane % LQ;
+    const int ml = lane / LQ;
+    const int q_index = blockIdx.x*LQ + qi;
+    const bool q_ok = q_index < nq;
+    const QState<M, VAR> qs(q, q_index, q_ok, values);
+    double acc2 = 0.0, acc1 = 0.0;
+    accumulate_rows<M, VAR>(qs, rows, warp*LM + ml, cnt, WARPS*LM, acc2, acc1);
+    reduce_block<LQ, WARPS, L::NOUT>(acc2, acc1, red);
     if (warp == 0 && ml == 0 && q_ok) {
-        double s2 = 0.0, s1v = 0.0;
-        #pragma unroll
-        for (int k = 0; k < WARPS; ++k) {
-            s2 += red[k][qi][0];
-            if constexpr (L::FQ1D) s1v += red[k][qi][1];
-        }
-        double *out = partial + (size_t)blockIdx.y*L::NOUT*nq;
         if constexpr (L::FQ1D) {
-            out[2*q_index] = s2;
-            out[2*q_index + 1] = s1v;
+            result[2*q_index] = accumulate ? result[2*q_index] + acc2 : acc2;
+            result[2*q_index + 1] = accumulate ? result[2*q_index + 1] + acc1 : acc1;
         } else {
-            out[q_index] = s2;
+            result[q_index] = accumulate ? result[q_index] + acc2 : acc2;
         }
     }
 }

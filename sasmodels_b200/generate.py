@@ -37,6 +37,12 @@ XY_CODES = {"qa": 1, "qac": 2, "qabc": 3, "qxy": 4}
 #: sasb200_<model>_<variant>_noalloc (csrc/sas_noalloc.cuh)
 NOALLOC_EXPORTS = {"cylinder": ("Iqxy", "sasb200::VAR_IQXY")}
 
+#: models with a hand-rearranged FP64 binding that hoists per-mesh-point work
+#: out of the q loop of one 2D form (header in csrc/, struct SasModelHoisted).
+#: Their library's sasb200_<model>_* entry points use it; the plugin's C as
+#: translated stays exported as sasb200_<model>_plugin_* for comparison.
+HOISTED_MODELS = {"cylinder": "fp64_hoisted.cuh"}
+
 _IQXY_RE = re.compile(r"(^|\s)double\s+I(?P<mode>q(ac|abc|xy))\s*[(]", re.M)
 _SHELL_RE = re.compile(r"(^|\s)double\s+shell_volume\s*[(]", re.M)
 _IDENT_RE = re.compile(r"(?<![.0-9A-Za-z_])([A-Za-z_][A-Za-z0-9_]*)")
@@ -374,13 +380,19 @@ def make_cuda_source(sm_info, sources):
     for fn in strfns:
         body.append(device_source(fn))
     body.append(model_struct(sm_info, table, xy_mode, have_shell))
+    hoisted = sm_info.id in HOISTED_MODELS
+    if hoisted:
+        body.append('#include "%s"' % HOISTED_MODELS[sm_info.id])
     body.append("}  // namespace sasm")
     f32c = f32c_block(sm_info.id, table, codes)
     if f32c:
         body.append(f32c)
     body.append('#include "sas_driver.cuh"')
     body.append('#include "sas_abi.cuh"')
-    body.append("SASB200_EXPORT_MODEL(%s, sasm::SasModel)" % sm_info.id)
+    main_binding = "sasm::SasModelHoisted" if hoisted else "sasm::SasModel"
+    body.append("SASB200_EXPORT_MODEL(%s, %s)" % (sm_info.id, main_binding))
+    if hoisted:
+        body.append("SASB200_EXPORT_MODEL(%s_plugin, sasm::SasModel)" % sm_info.id)
     if f32c:
         body.append("SASB200_EXPORT_MODEL(%s_f32c, sasm::SasModelF32c)" % sm_info.id)
         body.append('#include "sas_batch.cuh"')
@@ -388,10 +400,11 @@ def make_cuda_source(sm_info, sources):
     if sm_info.id in NOALLOC_EXPORTS:
         variant, var = NOALLOC_EXPORTS[sm_info.id]
         body.append('#include "sas_noalloc.cuh"')
-        body.append("SASB200_EXPORT_NOALLOC(%s, sasm::SasModel, %s, %s)"
-                    % (sm_info.id, variant, var))
+        body.append("SASB200_EXPORT_NOALLOC(%s, %s, %s, %s)"
+                    % (sm_info.id, main_binding, variant, var))
     meta = _mi.from_sasmodels(sm_info, xy_mode, have_shell)
     meta["f32c"] = bool(f32c)
+    meta["hoisted"] = hoisted
     return "\n".join(body) + "\n", meta
 
 

@@ -13,8 +13,8 @@ One process per GPU (torch.distributed) for the two ways the path shards:
   added in rank order, so every rank holds the same, reproducible total.
 
 The first two need no reduction on the data path -- the only collective is
-the final gather of results; the third has one small exchange (nout*nq + 4
-doubles per rank).
+the final gather of results, made on device tensors (gather_blocks); the
+third has one small exchange (nout*nq + 4 doubles per rank).
 
 Surrogate training runs data-parallel: identical replicas, each global
 batch split into equal contiguous slices (`batch_slice`), and one
@@ -71,22 +71,66 @@ def population_cost(model, sets):
     return costs
 
 
-def gather_in_order(local, indices, total):
-    """All-gather per-item results; returns the full list in item order on
-    every rank."""
+def _collective_device():
+    """Device the process group's collectives take tensors on: this rank's
+    CUDA device for NCCL, the host for gloo."""
+    import torch
     dist = _dist()
+    if dist.get_backend() == "nccl":
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cpu")
+
+
+def gather_blocks(block, group=None):
+    """All-gather one 1D float64 tensor per rank, of lengths that may differ
+    between ranks, into their concatenation in rank order on every rank.
+
+    Two collectives on device tensors (no host pickling): the lengths (one
+    int64 per rank), then the blocks padded to the longest.  Returns a tensor
+    on the collective device."""
+    import torch
+    dist = _dist()
+    size, _ = world()
+    dev = _collective_device() if size > 1 else block.device
+    block = block.reshape(-1).to(dev, torch.float64)
+    if size == 1:
+        return block
+    n = torch.tensor([block.numel()], dtype=torch.int64, device=dev)
+    counts = [torch.empty_like(n) for _ in range(size)]
+    dist.all_gather(counts, n, group=group)
+    counts = [int(c.item()) for c in counts]
+    width = max(max(counts), 1)
+    padded = torch.zeros(width, dtype=torch.float64, device=dev)
+    padded[:block.numel()] = block
+    bufs = [torch.empty_like(padded) for _ in range(size)]
+    dist.all_gather(bufs, padded, group=group)
+    return torch.cat([b[:c] for b, c in zip(bufs, counts)])
+
+
+def gather_in_order(local, indices, total):
+    """All-gather per-item result arrays (1D, any lengths); returns the full
+    list in item order on every rank, as numpy arrays.  The arrays travel as
+    one flat device tensor per rank with a small table of item indices and
+    lengths (gather_blocks), not as pickled host objects."""
+    import torch
     size, _ = world()
     if size == 1:
         out = [None]*total
         for i, v in zip(indices, local):
-            out[i] = v
+            out[i] = np.asarray(v.cpu() if isinstance(v, torch.Tensor) else v)
         return out
-    pieces = [None]*size
-    dist.all_gather_object(pieces, (list(indices), list(local)))
+    dev = _collective_device()
+    arrays = [torch.as_tensor(v, dtype=torch.float64).reshape(-1).to(dev) for v in local]
+    flat = torch.cat(arrays) if arrays else torch.zeros(0, dtype=torch.float64, device=dev)
+    table = torch.tensor([x for i, a in zip(indices, arrays) for x in (i, a.numel())],
+                         dtype=torch.float64, device=dev)
+    all_table = gather_blocks(table).cpu().numpy().astype(np.int64).reshape(-1, 2)
+    all_flat = gather_blocks(flat).cpu().numpy()
     out = [None]*total
-    for idx, vals in pieces:
-        for i, v in zip(idx, vals):
-            out[i] = v
+    off = 0
+    for i, n in all_table:
+        out[int(i)] = all_flat[off:off + n]
+        off += n
     return out
 
 
@@ -119,21 +163,29 @@ def q_blocks(nq, nranks):
     return [(int(b[r]), int(b[r + 1])) for r in range(nranks)]
 
 
-def evaluate_image(q_vectors, evaluate):
+def evaluate_image(q_vectors, evaluate, nout=1):
     """One image split by q blocks: *evaluate(q_block_vectors)* returns the
-    raw result (F^2 slots then the 4 norms) of its block; returns the full
-    raw vector (q slots in caller order, norms of rank 0) on every rank."""
+    raw result of its block (nout*nq_block slots, then the 4 norms; a numpy
+    array or torch tensor); returns the full raw vector (q slots in caller
+    order, norms of rank 0) on every rank as a numpy array.  *nout* is 2 for
+    1D models returning <F> and <F^2>, else 1: it comes from the model, not
+    from the block, so a rank with an empty block (nq < ranks) still
+    assembles the image right.  The blocks travel as device tensors
+    (gather_blocks)."""
+    import torch
     size, rank = world()
     nq = len(q_vectors[0])
     lo, hi = q_blocks(nq, size)[rank]
-    raw = np.asarray(evaluate([np.asarray(v)[lo:hi] for v in q_vectors]))
-    nout = (len(raw) - 4)//max(hi - lo, 1) if hi > lo else 1
-    pieces = gather_in_order([raw], [rank], size)
-    out = []
-    for r, piece in enumerate(pieces):
-        a, b = q_blocks(nq, size)[r]
-        out.append(piece[:nout*(b - a)])
-    return np.concatenate(out + [pieces[0][-4:]])
+    raw = evaluate([np.asarray(v)[lo:hi] for v in q_vectors])
+    raw = torch.as_tensor(raw, dtype=torch.float64).reshape(-1)
+    # every rank takes both collectives, a malformed block included, and
+    # only then reports it, so the other ranks are not left waiting
+    slots = gather_blocks(raw[:nout*(hi - lo)])
+    norms = gather_blocks(raw[nout*(hi - lo):])[:4]      # rank 0's four norms
+    if raw.numel() != nout*(hi - lo) + 4:
+        raise ValueError("block result has %d values, expected %d"
+                         % (raw.numel(), nout*(hi - lo) + 4))
+    return torch.cat([slots, norms]).cpu().numpy()
 
 
 def mesh_ranges(num_eval, nranks):

@@ -170,8 +170,9 @@ def test_abi_rejects_bad_arguments_without_gpu():
         lib.call("Iq", 10, 0, 3, None, 1, 1, 1, 0.0, 0, 1, 1 << 20, 0, None)
     with pytest.raises(RuntimeError, match="tile"):
         lib.call("Iq", 10, 0, 3, 1, 1, 1, 1, 0.0, 0, 1, 1 << 20, 0x10307, None)
+    # a mesh range above the single-launch limit needs a workspace
     with pytest.raises(RuntimeError, match="workspace"):
-        lib.call("Iq", 10, 0, 3, 1, 1, 1, 1, 0.0, 0, 1, 16, 0, None)
+        lib.call("Iq", 10, 0, 100000, 1, 1, 1, 1, 0.0, 0, 1, 16, 0, None)
 
 
 def test_line_form_refuses_orientation_dispersion():

@@ -63,7 +63,12 @@ def _worker(rank, size, port, queue):
         mesh = multigpu.evaluate_mesh(
             d1.num_eval, lambda lo, hi: dll.call("Iq", q1, d1.buffer, v1, 2, pd_start=lo,
                                                  pd_stop=hi, result=np.zeros(2*len(q1) + 4)))
-        queue.put((rank, [c.tolist() for c in curves], raw.tolist(), mesh.tolist()))
+        # a 1D image returning <F> and <F^2> (nout = 2) with fewer q points
+        # than ranks: rank 1's block is empty
+        tiny = multigpu.evaluate_image(
+            [q1[:1]], lambda qb: reference_raw(name1, info1, qb, pars1), nout=2)
+        queue.put((rank, [c.tolist() for c in curves], raw.tolist(), mesh.tolist(),
+                   tiny.tolist()))
     finally:
         dist.destroy_process_group()
 
@@ -101,8 +106,10 @@ def test_two_rank_gloo_matches_single_process():
     raw_single = reference_raw(name, load_info(name), qv, pars)
     name1, (q1,), pars1 = workloads.sphere_1d()
     mesh_single = reference_raw(name1, load_info(name1), [q1], pars1)
+    tiny_single = reference_raw(name1, load_info(name1), [q1[:1]], pars1)
     meshes = []
-    for rank, curves, raw, mesh in results:
+    for rank, curves, raw, mesh, tiny in results:
+        np.testing.assert_array_equal(np.array(tiny), tiny_single)
         assert len(curves) == len(single)
         for a, b in zip(curves, single):
             np.testing.assert_array_equal(np.array(a), b)
