@@ -1,10 +1,15 @@
 """
-Parameter dict -> dispersity mesh -> kernel call.
+Parameter dict -> dispersity mesh -> kernel call, for callers that run
+without the sasmodels package (with it installed, ``install()`` lets the
+reference's own ``sasmodels.direct_model`` drive the B200 kernels).
 
-Same call path as ``sasmodels/direct_model.py:41-154``: a caller that used
-``sasmodels.direct_model.call_kernel(kernel, pars)`` with a DLL kernel gets
-the same mesh, the same packed arrays and so the same integral from a
-:class:`sasmodels_b200.kernel.B200Kernel`.
+The mesh must be the one the reference builds for the same dict
+(``sasmodels/direct_model.py:41-154``): one (value, points, weights) entry
+per call parameter, in the table's order; a parameter is polydisperse only
+if it may be (``polydisperse``), is active for the kernel's dimension
+(``pd_1d``/``pd_2d``) and has both points and a width; an idle orientation
+parameter contributes a single point at zero jitter (its value is the view
+angle, the jitter is the distribution); unknown names are an error.
 """
 
 from . import weights
@@ -14,22 +19,30 @@ from .details import make_kernel_args
 #: (``sasmodels/product.py:143``).
 RADIUS_MODE_ID = "radius_effective_mode"
 
+#: dispersity entries of a parameter `p`: p_pd, p_pd_n, p_pd_nsigma, p_pd_type
+_PD_SUFFIXES = ("_pd", "_pd_n", "_pd_nsigma", "_pd_type")
+
 
 def call_kernel(calculator, pars, cutoff=0., mono=False):
-    """I(q) for *pars* (``direct_model.py:41-59``)."""
-    mesh = get_mesh(calculator.info, pars, dim=calculator.dim, mono=mono)
-    call_details, values, is_magnetic = make_kernel_args(calculator, mesh)
-    return calculator(call_details, values, cutoff, is_magnetic)
+    """I(q) of *calculator* (a kernel from ``make_kernel``) for the
+    parameter dict *pars*."""
+    call_details, values, magnetic = _marshal(calculator, pars, mono)
+    return calculator(call_details, values, cutoff, magnetic)
 
 
 def call_Fq(calculator, pars, cutoff=0., mono=False):
-    """(F1, F2, R_eff, V_shell, V_form/V_shell) for *pars*
-    (``direct_model.py:61-77``)."""
+    """(<F>, <F^2>, R_eff, V_shell, V_form/V_shell) for *pars*; the entry
+    ``radius_effective_mode`` of *pars* selects the effective radius
+    (default 1)."""
     pars = dict(pars)
-    R_eff_type = int(pars.pop(RADIUS_MODE_ID, 1.0))
+    mode = int(pars.pop(RADIUS_MODE_ID, 1.0))
+    call_details, values, magnetic = _marshal(calculator, pars, mono)
+    return calculator.Fq(call_details, values, cutoff, magnetic, mode)
+
+
+def _marshal(calculator, pars, mono):
     mesh = get_mesh(calculator.info, pars, dim=calculator.dim, mono=mono)
-    call_details, values, is_magnetic = make_kernel_args(calculator, mesh)
-    return calculator.Fq(call_details, values, cutoff, is_magnetic, R_eff_type)
+    return make_kernel_args(calculator, mesh)
 
 
 class _CallShape:
@@ -54,47 +67,44 @@ def make_call_args(model_info, pars, q_vectors, mono=False):
 
 
 def get_mesh(model_info, values, dim='1d', mono=False):
-    """
-    One (value, dispersity, weights) tuple per call parameter; parameters not
-    active for *dim* are monodisperse (``direct_model.py:97-124``).
-    """
-    parameters = model_info.parameters
+    """[(value, points, weights)] for every call parameter of *model_info*,
+    from the dict *values*; *dim* ('1d', '2d', or anything else for all
+    polydisperse parameters) picks which dispersities are active, *mono*
+    switches them all off."""
+    table = model_info.parameters
+    known = set()
+    for p in table.call_parameters:
+        known.add(p.name)
+        if p.polydisperse:
+            known.update(p.name + sfx for sfx in _PD_SUFFIXES)
+    unused = [k for k in values if k not in known]
+    if unused:
+        raise TypeError("Unused parameters in call: %s" % ", ".join(unused))
     if mono:
-        active = lambda name: False
+        active = ()
     elif dim == '1d':
-        active = lambda name: name in parameters.pd_1d
+        active = table.pd_1d
     elif dim == '2d':
-        active = lambda name: name in parameters.pd_2d
+        active = table.pd_2d
     else:
-        active = lambda name: True
-    values = dict(values)
-    mesh = [_pop_par_weights(p, values, active(p.name))
-            for p in parameters.call_parameters]
-    if values:
-        raise TypeError(f"Unused parameters in call: {', '.join(values.keys())}")
-    return mesh
+        active = None          # every polydisperse parameter
+    return [_parameter_mesh(p, values, active is None or p.name in active)
+            for p in table.call_parameters]
 
 
-def _pop_par_weights(parameter, values, active=True):
-    """
-    Distribution for one parameter from name, name_pd, name_pd_n,
-    name_pd_nsigma and name_pd_type, defaulting to n=0, nsigma=3, gaussian
-    (``direct_model.py:127-154``).
-    """
-    value = float(values.pop(parameter.name, parameter.default))
-    if parameter.polydisperse:
-        npts = values.pop(parameter.name+'_pd_n', 0)
-        width = values.pop(parameter.name+'_pd', 0.0)
-        nsigma = values.pop(parameter.name+'_pd_nsigma', 3.0)
-        distribution = values.pop(parameter.name+'_pd_type', 'gaussian')
-        relative = parameter.relative_pd
-        if npts == 0 or width == 0.0 or not active:
-            # Orientation parameters carry the view angle as the value and the
-            # jitter in the distribution, so an idle jitter is 0, not the angle.
-            pd = [value if relative else 0.0], [1.0]
-        else:
-            pd = weights.get_weights(distribution, npts, width, nsigma,
-                                     value, parameter.limits, relative)
-    else:
-        pd = [value], [1.0]
-    return value, pd[0], pd[1]
+def _parameter_mesh(p, values, active):
+    """(value, points, weights) of call parameter *p* from its entries in
+    *values* (defaults: the table's value, no points, width 0, 3 sigmas,
+    gaussian)."""
+    value = float(values.get(p.name, p.default))
+    if not p.polydisperse:
+        return value, [value], [1.0]
+    npts = values.get(p.name + "_pd_n", 0)
+    width = values.get(p.name + "_pd", 0.0)
+    if not active or npts == 0 or width == 0.0:
+        # idle: the value itself, or for orientation jitter no jitter
+        return value, [value if p.relative_pd else 0.0], [1.0]
+    points, wts = weights.get_weights(values.get(p.name + "_pd_type", "gaussian"), npts,
+                                      width, values.get(p.name + "_pd_nsigma", 3.0), value,
+                                      p.limits, p.relative_pd)
+    return value, points, wts

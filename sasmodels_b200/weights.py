@@ -1,164 +1,121 @@
 """
-Dispersity distributions: parameter value -> (mesh values, normalised weights).
+Dispersity meshes: a parameter's value and distribution -> (points, weights).
 
-Same distributions, defaults and truncation rules as the sasmodels plugin API
-(``sasmodels/weights.py``): the kernels consume the weight vectors these
-produce, so the points and weights must be identical for the DLL and the B200
-path to integrate over the same mesh.
+The kernels integrate over the points and weights given here, so they must
+be the ones the reference's plugin API produces (``sasmodels/weights.py``:
+distributions :86-220, defaults and truncation :21-83, normalisation
+:264-291), bit for bit: each weight function below evaluates the same
+expression as the reference's in the same operation order, on points from
+the same ``numpy.linspace`` call.  The organisation is this module's own: a
+table of distribution specs (default size and width in sigmas, node rule,
+weight function, domain) over two node rules, and one function that applies
+a spec.
+
+Volume-type parameters take a width relative to their value; orientation
+jitter is absolute and centred on zero.  A distribution of zero width (or
+fewer than two points) is its centre alone, if the centre lies within the
+parameter's limits.  Points outside the limits are dropped.
 """
 
-from collections import OrderedDict
+from collections import namedtuple
 
 import numpy as np
 from scipy.special import gammaln
 
-
-class Dispersion:
-    """Base distribution (``weights.py:21-83``)."""
-    type = "base disperser"
-    default = dict(npts=35, width=0, nsigmas=3)
-
-    def __init__(self, npts=None, width=None, nsigmas=None):
-        self.npts = self.default['npts'] if npts is None else int(npts)
-        self.width = self.default['width'] if width is None else width
-        self.nsigmas = self.default['nsigmas'] if nsigmas is None else nsigmas
-
-    def get_weights(self, center, lb, ub, relative):
-        """
-        Values and (unnormalised) weights.  Volume parameters use a width
-        relative to *center*; orientation jitter is absolute and centred on
-        zero (``weights.py:50-72``).
-        """
-        sigma = self.width*center if relative else self.width
-        if not relative:
-            center = 0
-        if sigma == 0 or self.npts < 2:
-            if lb <= center <= ub:
-                return np.array([center], 'd'), np.array([1.], 'd')
-            return np.array([], 'd'), np.array([], 'd')
-        return self._weights(center, sigma, lb, ub)
-
-    def _weights(self, center, sigma, lb, ub):
-        raise NotImplementedError
-
-    def _linspace(self, center, sigma, lb, ub):
-        """npts evenly spaced over +/- nsigmas, clipped to [lb, ub]
-        (``weights.py:78-83``)."""
-        x = center + np.linspace(-self.nsigmas*sigma, +self.nsigmas*sigma,
-                                 self.npts)
-        return x[(x >= lb) & (x <= ub)]
+# ------------------------------------------------------------ node rules ---
 
 
-class GaussianDispersion(Dispersion):
-    """``weights.py:86-102``"""
-    type = "gaussian"
-    default = dict(npts=35, width=0, nsigmas=3)
-
-    def _weights(self, center, sigma, lb, ub):
-        x = self._linspace(center, sigma, lb, ub)
-        return x, np.exp((x-center)**2 / (-2.0*sigma*sigma))
+def _nodes_sigma(center, sigma, npts, nsigmas):
+    """npts points evenly spaced over center +/- nsigmas*sigma."""
+    return center + np.linspace(-nsigmas*sigma, +nsigmas*sigma, npts)
 
 
-class UniformDispersion(Dispersion):
-    """``weights.py:104-117``"""
-    type = "uniform"
-    default = dict(npts=35, width=0, nsigmas=None)
-
-    def _weights(self, center, sigma, lb, ub):
-        x = np.linspace(center-sigma, center+sigma, self.npts)
-        x = x[(x >= lb) & (x <= ub)]
-        return x, np.ones_like(x)
+def _nodes_width(center, sigma, npts, nsigmas):
+    """npts points evenly spaced over center +/- sigma (nsigmas unused)."""
+    return np.linspace(center - sigma, center + sigma, npts)
 
 
-class RectangleDispersion(Dispersion):
-    """``weights.py:119-132``"""
-    type = "rectangle"
-    default = dict(npts=35, width=0, nsigmas=1.73205)
+# ------------------------------------------------------ weight functions ---
+# Unnormalised densities at the points x for a distribution of centre c and
+# width s (the expressions of sasmodels/weights.py, operation by operation).
 
-    def _weights(self, center, sigma, lb, ub):
-        x = self._linspace(center, sigma, lb, ub)
-        x = x[np.fabs(x-center) <= np.fabs(sigma)*np.sqrt(3.0)]
-        return x, np.ones_like(x)
+def _w_gaussian(x, c, s):
+    return np.exp((x - c)**2 / (-2.0*s*s))
 
 
-class LogNormalDispersion(Dispersion):
-    """``weights.py:134-149``"""
-    type = "lognormal"
-    default = dict(npts=80, width=0, nsigmas=8)
-
-    def _weights(self, center, sigma, lb, ub):
-        x = self._linspace(center, sigma, max(lb, 1e-8), max(ub, 1e-8))
-        sig = np.fabs(sigma/center)
-        px = np.exp(-0.5*((np.log(x)-np.log(center))/sig)**2)/(x*sig)
-        return x, px
+def _w_flat(x, c, s):
+    return np.ones_like(x)
 
 
-class SchulzDispersion(Dispersion):
-    """``weights.py:152-176``"""
-    type = "schulz"
-    default = dict(npts=80, width=0, nsigmas=8)
-
-    def _weights(self, center, sigma, lb, ub):
-        x = self._linspace(center, sigma, max(lb, 1e-8), max(ub, 1e-8))
-        R = x/center
-        z = (center/sigma)**2
-        arg = z*np.log(z) + (z-1)*np.log(R) - R*z - np.log(center) - gammaln(z)
-        return x, np.exp(arg)
+def _w_lognormal(x, c, s):
+    sig = np.fabs(s/c)
+    return np.exp(-0.5*((np.log(x) - np.log(c))/sig)**2)/(x*sig)
 
 
-class ArrayDispersion(Dispersion):
-    """``weights.py:179-205``"""
-    type = "array"
-    default = dict(npts=35, width=0, nsigmas=1)
-
-    def __init__(self, npts=None, width=None, nsigmas=None):
-        Dispersion.__init__(self, npts, width, nsigmas)
-        self.values = np.array([0.], 'd')
-        self.weights = np.array([1.], 'd')
-
-    def set_weights(self, values, weights):
-        self.values = np.ascontiguousarray(values, 'd')
-        self.weights = np.ascontiguousarray(weights, 'd')
-        self.npts = len(values)
-
-    def _weights(self, center, sigma, lb, ub):
-        idx = (self.values >= lb) & (self.values <= ub)
-        return self.values[idx], self.weights[idx]
+def _w_schulz(x, c, s):
+    R = x/c
+    z = (c/s)**2
+    return np.exp(z*np.log(z) + (z - 1)*np.log(R) - R*z - np.log(c) - gammaln(z))
 
 
-class BoltzmannDispersion(Dispersion):
-    """``weights.py:207-220``"""
-    type = "boltzmann"
-    default = dict(npts=35, width=0, nsigmas=3)
-
-    def _weights(self, center, sigma, lb, ub):
-        x = self._linspace(center, sigma, lb, ub)
-        return x, np.exp(-np.abs(x-center) / np.abs(sigma))
+def _w_boltzmann(x, c, s):
+    return np.exp(-np.abs(x - c) / np.abs(s))
 
 
-#: name -> distribution class, in the order sasview lists them
-#: (``weights.py:225-233``).
-DISTRIBUTIONS = OrderedDict((d.type, d) for d in (
-    RectangleDispersion,
-    UniformDispersion,
-    ArrayDispersion,
-    LogNormalDispersion,
-    GaussianDispersion,
-    SchulzDispersion,
-    BoltzmannDispersion,
-))
-MODELS = DISTRIBUTIONS
+#: npts, nsigmas: defaults; nodes: node rule; weight: density;
+#: positive: points are taken over [max(lb, 1e-8), max(ub, 1e-8)] (the
+#: densities with a log); box: also drop points farther than |s| sqrt(3)
+#: from the centre (the rectangle of standard deviation s)
+Spec = namedtuple("Spec", "npts nsigmas nodes weight positive box")
+
+SPECS = {
+    "gaussian": Spec(35, 3, _nodes_sigma, _w_gaussian, False, False),
+    "uniform": Spec(35, None, _nodes_width, _w_flat, False, False),
+    "rectangle": Spec(35, 1.73205, _nodes_sigma, _w_flat, False, True),
+    "lognormal": Spec(80, 8, _nodes_sigma, _w_lognormal, True, False),
+    "schulz": Spec(80, 8, _nodes_sigma, _w_schulz, True, False),
+    "boltzmann": Spec(35, 3, _nodes_sigma, _w_boltzmann, False, False),
+}
+
+#: distribution names in the order the reference lists them
+#: (sasmodels/weights.py:225-233); "array" (user-supplied points and
+#: weights) is handled by the caller, not by get_weights
+NAMES = ("rectangle", "uniform", "array", "lognormal", "gaussian", "schulz", "boltzmann")
 
 
-def get_weights(disperser, n, width, nsigmas, value, limits, relative):
-    """
-    (values, weights) for one polydisperse parameter with weights normalised
-    to sum to one (``weights.py:264-291``).
-    """
-    if disperser == "array":
-        raise NotImplementedError("Don't handle arrays through get_weights;"
-                                  " use values and weights directly")
-    cls = DISTRIBUTIONS[disperser]
-    obj = cls(n, width, nsigmas)
-    v, w = obj.get_weights(value, limits[0], limits[1], relative)
-    return v, w/np.sum(w)
+def dispersion(kind, npts, width, nsigmas, center, limits, relative):
+    """Unnormalised (points, weights) of distribution *kind* for a
+    parameter at *center* with *limits* = (lb, ub).  *npts*, *width* and
+    *nsigmas* may be None for the distribution's defaults (width 0)."""
+    if kind == "array":
+        raise ValueError("array dispersity: pass the points and weights directly")
+    try:
+        spec = SPECS[kind]
+    except KeyError:
+        raise ValueError("unknown dispersity distribution %r" % (kind,)) from None
+    npts = spec.npts if npts is None else int(npts)
+    width = 0 if width is None else width
+    nsigmas = spec.nsigmas if nsigmas is None else nsigmas
+    lb, ub = limits
+    sigma = width*center if relative else width
+    if not relative:
+        center = 0
+    if sigma == 0 or npts < 2:
+        if lb <= center <= ub:
+            return np.array([center], 'd'), np.array([1.], 'd')
+        return np.array([], 'd'), np.array([], 'd')
+    if spec.positive:
+        lb, ub = max(lb, 1e-8), max(ub, 1e-8)
+    x = spec.nodes(center, sigma, npts, nsigmas)
+    x = x[(x >= lb) & (x <= ub)]
+    if spec.box:
+        x = x[np.fabs(x - center) <= np.fabs(sigma)*np.sqrt(3.0)]
+    return x, spec.weight(x, center, sigma)
+
+
+def get_weights(kind, npts, width, nsigmas, value, limits, relative):
+    """(points, weights) of one polydisperse parameter, the weights
+    normalised to sum to one (the call the reference's direct_model makes,
+    sasmodels/weights.py:264-291)."""
+    x, w = dispersion(kind, npts, width, nsigmas, value, limits, relative)
+    return x, w/np.sum(w)
