@@ -225,7 +225,7 @@ def _pack_lib():
         raise RuntimeError("device packer not built: %s" % path)
     lib = ct.CDLL(path)
     P, I = ct.c_void_p, ct.c_int32
-    lib.sasb200_pack_values.argtypes = [I, I, I] + [P]*8 + [P]
+    lib.sasb200_pack_values.argtypes = [I, I, I, I] + [P]*12 + [P]
     lib.sasb200_pack_values.restype = I
     lib.sasb200_pack_max_pars.restype = I
     lib.sasb200_pack_last_error.restype = ct.c_char_p
@@ -255,9 +255,12 @@ class _Packer:
         host_rows = sorted(ca["host_values"])
         dev_off[host_rows] = -1
         f64 = dict(dtype=torch.float64)
+        self.nmag = int(ca["nmag"])
         self.h_table = torch.empty(n*(nvalues + 2*npars), **f64).pin_memory()
         self.d_table = torch.empty_like(self.h_table, device=device)
-        self.d_npts = torch.as_tensor(ca["npts"].ravel(), device=device)
+        # int32 table: npts, first, ntot, kinds (n x npars each), magnetic (n)
+        self.h_itable = torch.empty(4*n*npars + n, dtype=torch.int32).pin_memory()
+        self.d_itable = torch.empty_like(self.h_itable, device=device)
         self.d_flags = torch.as_tensor(ca["flags"], device=device)
         self.d_off = torch.as_tensor(dev_off, device=device)
         self.d_size = torch.as_tensor(sizes, device=device)
@@ -271,6 +274,11 @@ class _Packer:
         t[:a] = ca["scalars"].ravel()
         t[a:b] = ca["widths"].ravel()
         t[b:] = ca["nsigmas"].ravel()
+        it = self.h_itable.numpy()
+        m = self.n*self.npars
+        for j, key in enumerate(("npts", "first", "ntot", "kinds")):
+            it[j*m:(j + 1)*m] = ca[key].ravel()
+        it[4*m:] = ca["magnetic"]
         for r, buf in self.h_rows.items():
             buf.numpy()[:] = ca["host_values"][r]
 
@@ -280,16 +288,20 @@ class _Packer:
         torch = self.torch
         with torch.cuda.stream(self.stream):
             self.d_table.copy_(self.h_table, non_blocking=True)
+            self.d_itable.copy_(self.h_itable, non_blocking=True)
             for r, buf in self.h_rows.items():
                 o = int(self.offs[r])
                 d_val[o:o + buf.numel()].copy_(buf, non_blocking=True)
         a = self.n*self.nvalues
         b = a + self.n*self.npars
         base = self.d_table.data_ptr()
+        ib = self.d_itable.data_ptr()
+        m = 4*self.n*self.npars
         status = self.lib.sasb200_pack_values(
-            self.n, self.nvalues, self.npars, base, base + 8*a, base + 8*b,
-            self.d_npts.data_ptr(), self.d_flags.data_ptr(), self.d_off.data_ptr(),
-            self.d_size.data_ptr(), d_val.data_ptr(), self.stream.cuda_stream)
+            self.n, self.nvalues, self.npars, self.nmag, base, base + 8*a, base + 8*b,
+            ib, ib + m, ib + 2*m, ib + 3*m, self.d_flags.data_ptr(), ib + 4*m,
+            self.d_off.data_ptr(), self.d_size.data_ptr(), d_val.data_ptr(),
+            self.stream.cuda_stream)
         if status != 0:
             raise RuntimeError("pack_values failed (%d): %s"
                                % (status, self.lib.sasb200_pack_last_error().decode()))
@@ -451,6 +463,7 @@ class Population:
         old = self.columns
         if (not np.array_equal(ca["det"], old["det"])
                 or not np.array_equal(ca["val_sizes"], old["val_sizes"])
+                or not np.array_equal(ca["magnetic"], old["magnetic"])
                 or set(ca["host_values"]) != set(old["host_values"])):
             raise ValueError("the population changed its dispersity structure")
         self.stream.synchronize()

@@ -14,6 +14,10 @@ elementwise (``np.linspace`` with array end points, the same exponent, one
 ``make_call_args`` returns for that set, bit for bit; sets the array path
 does not cover (distributions other than gaussian, points clipped at a
 parameter limit, vector parameters) go through ``make_call_args`` itself.
+
+``column_args`` prepares a population given as parameter columns for the
+device packer (``csrc/pack.cu``), which expands every distribution, clipped
+meshes and the magnetic conversion on the GPU.
 """
 
 import numpy as np
@@ -145,6 +149,37 @@ def _column(columns, name, default, n):
     return v
 
 
+#: distribution codes of the device packer (csrc/pack.cu, enum Kind)
+KIND_CODES = {"gaussian": 0, "uniform": 1, "rectangle": 2, "lognormal": 3, "schulz": 4,
+              "boltzmann": 5}
+
+
+def _kept_ranges(kind, center, sigma, nsig, npts, limits):
+    """For the sets of one parameter sharing distribution `kind` and point
+    count `npts`: the linspace points of weights.dispersion (the same
+    arithmetic, vectorised over rows), which of them the limits (and the
+    rectangle's box) keep, and whether they form one contiguous index range.
+    Returns (first, count, contiguous)."""
+    from .weights import SPECS, _nodes_width
+    spec = SPECS[kind]
+    if spec.nodes is _nodes_width:
+        x = np.linspace(center - sigma, center + sigma, npts, axis=1)
+    else:
+        x = center[:, None] + np.linspace(-nsig*sigma, +nsig*sigma, npts, axis=1)
+    lb, ub = limits
+    if spec.positive:
+        lb, ub = max(lb, 1e-8), max(ub, 1e-8)
+    keep = (x >= lb) & (x <= ub)
+    if spec.box:
+        keep &= np.fabs(x - center[:, None]) <= np.fabs(sigma)[:, None]*np.sqrt(3.0)
+    count = keep.sum(axis=1)
+    first = np.argmax(keep, axis=1)
+    idx = np.arange(npts)[None, :]
+    contiguous = np.all(keep == ((idx >= first[:, None]) & (idx < (first + count)[:, None])),
+                        axis=1)
+    return first, count, contiguous
+
+
 def column_args(info, n_sets, columns, dim="1d"):
     """
     Marshaling of a population given as parameter columns, for the device
@@ -154,15 +189,20 @@ def column_args(info, n_sets, columns, dim="1d"):
     per set; parameters not named keep their defaults.
 
     Returns a dict with the compact per-set table the device expands
-    (``scalars`` [n, nvalues], ``widths``/``nsigmas`` [n, npars], ``npts``
-    [n, npars] with 0 for an idle parameter, ``flags`` [npars]), the
+    (``scalars`` [n, nvalues], ``widths``/``nsigmas`` [n, npars]; per set
+    and kernel parameter ``npts`` the kept points (0 for an idle parameter),
+    ``first`` the index of the first kept point among the ``ntot`` points of
+    its linspace, ``kinds`` the distribution code; ``flags`` [npars];
+    ``magnetic`` [n] whether the set's magnetic moments are converted), the
     ``details`` object, ``det`` buffer, ``num_eval`` and padded ``val_sizes``
     of every set, and ``host_values`` {set: values} for the sets the table
-    cannot describe (a point clipped at a parameter limit, a dispersity
-    other than gaussian, fewer than 2 points, a zero sigma, a magnetic
-    moment), which ``make_call_args`` marshals.  A device-packed set's values
-    equal ``make_call_args``'s except for the exp of its weights (an ulp or
-    two).
+    cannot describe (a zero sigma, fewer than two points, an empty or split
+    range of kept points, an "array" dispersity, a lognormal or schulz
+    jitter centred on zero), which ``make_call_args`` marshals.  Every
+    distribution of the plugin API and the magnetic conversion run on the
+    device; a device-packed set's values equal ``make_call_args``'s points
+    bit for bit, its weights and magnetic components to an ulp or two
+    (exp, log, lgamma, sin, cos).
     """
     table = info.parameters
     npars = table.npars
@@ -184,6 +224,9 @@ def column_args(info, n_sets, columns, dim="1d"):
     widths = np.zeros((n, npars))
     nsigmas = np.full((n, npars), 3.0)
     npts = np.zeros((n, npars), np.int32)
+    first = np.zeros((n, npars), np.int32)
+    ntot = np.zeros((n, npars), np.int32)
+    kinds = np.zeros((n, npars), np.int32)
     lengths = np.ones((n, npars), np.int64)
     flags = np.array([(1 if p.relative_pd else 0) | (2 if (p.relative_pd or not p.polydisperse)
                                                      else 0) for p in kpars], np.int32)
@@ -199,18 +242,34 @@ def column_args(info, n_sets, columns, dim="1d"):
         value = scalars[:, NUM_COMMON_PARS + k]
         sigma = w*value if p.relative_pd else w
         center = value if p.relative_pd else np.zeros(n)
-        ends = np.stack([center + (-ns)*sigma, center + ns*sigma])
-        lb, ub = p.limits
-        inside = (ends.min(axis=0) >= lb) & (ends.max(axis=0) <= ub)
-        simple = (kind == "gaussian") & (nn >= 2) & (sigma != 0) & inside
-        host |= dispersed & ~simple
-        npts[:, k] = np.where(dispersed, nn, 0)
-        widths[:, k] = np.where(dispersed, w, 0.0)
+        code = np.array([KIND_CODES.get(str(t), -1) for t in kind], np.int32)
+        ok = dispersed & (code >= 0) & (nn >= 2) & (sigma != 0)
+        # a zero linspace step takes numpy's other formula, for every row of
+        # a vectorised call: such sets go the scalar way
+        ok &= (code == KIND_CODES["uniform"]) | (ns != 0)
+        if not p.relative_pd:
+            ok &= (code != KIND_CODES["lognormal"]) & (code != KIND_CODES["schulz"])
+        cnt = np.zeros(n, np.int64)
+        fst = np.zeros(n, np.int64)
+        for name, c in KIND_CODES.items():
+            for m in np.unique(nn[ok & (code == c)]):
+                rows = np.nonzero(ok & (code == c) & (nn == m))[0]
+                f0, c0, contiguous = _kept_ranges(name, center[rows], sigma[rows],
+                                                  ns[rows], int(m), p.limits)
+                fst[rows], cnt[rows] = f0, c0
+                ok[rows] &= contiguous & (c0 > 0)
+        host |= dispersed & ~ok
+        npts[:, k] = np.where(ok, cnt, 0)
+        first[:, k] = np.where(ok, fst, 0)
+        ntot[:, k] = np.where(ok, nn, 0)
+        kinds[:, k] = np.where(ok, code, 0)
+        widths[:, k] = np.where(ok, w, 0.0)
         nsigmas[:, k] = ns
-        lengths[:, k] = np.where(dispersed, nn, 1)
+        lengths[:, k] = np.where(ok, cnt, 1)
+    magnetic = np.zeros(n, np.int32)
     if table.nmagnetic:
         mag = scalars[:, table.nvalues - NUM_MAGNETIC_PARS*table.nmagnetic:]
-        host |= np.any(mag[:, ::NUM_MAGNETIC_PARS] != 0.0, axis=1)
+        magnetic[:] = np.any(mag[:, ::NUM_MAGNETIC_PARS] != 0.0, axis=1)
     det_len = 4*table.max_pd + 4
     det = np.empty((n, det_len), np.int32)
     num_eval = np.empty(n, np.int64)
@@ -244,7 +303,8 @@ def column_args(info, n_sets, columns, dim="1d"):
         val_sizes[r] = values.size
         details[r] = d
         host_values[int(r)] = values
-    return dict(scalars=scalars, widths=widths, nsigmas=nsigmas, npts=npts, flags=flags,
+    return dict(scalars=scalars, widths=widths, nsigmas=nsigmas, npts=npts, first=first,
+                ntot=ntot, kinds=kinds, flags=flags, magnetic=magnetic, nmag=table.nmagnetic,
                 lengths=lengths, details=details, det=det, num_eval=num_eval,
                 val_sizes=val_sizes, host_values=host_values)
 

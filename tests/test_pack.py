@@ -13,9 +13,14 @@ from oracle import pack_ref
 MODELS = ["cylinder", "ellipsoid", "core_shell_cylinder", "sphere", "core_shell_sphere"]
 
 
-def _columns(info, n, seed, clip=True, other_types=True):
+KINDS = ["gaussian", "lognormal", "schulz", "uniform", "rectangle", "boltzmann"]
+
+
+def _columns(info, n, seed, clip=True, other_types=True, magnetic=False):
     """A random population as columns: values per set, dispersity widths,
-    point counts and (sometimes) other distributions per set."""
+    point counts and (with other_types) every distribution per set; with
+    clip, widths that push points past a parameter limit; with magnetic,
+    magnetic moments on some sets."""
     rng = np.random.default_rng(seed)
     cols = {}
     for p in info.parameters.kernel_parameters:
@@ -31,16 +36,25 @@ def _columns(info, n, seed, clip=True, other_types=True):
         width = rng.uniform(0.0, 0.35, n)
         width[rng.uniform(size=n) < 0.2] = 0.0
         cols[p.name + "_pd"] = width if p.type != "orientation" else rng.uniform(0, 15, n)
-        cols[p.name + "_pd_n"] = rng.choice([0, 1, 5, 35], n)
+        cols[p.name + "_pd_n"] = rng.choice([0, 1, 5, 35], n, p=[0.3, 0.04, 0.3, 0.36])
         if other_types and p.type != "orientation":
-            kinds = np.array(["gaussian"]*n, dtype=object)
-            kinds[::11] = "lognormal"
-            cols[p.name + "_pd_type"] = kinds
+            cols[p.name + "_pd_type"] = np.array([KINDS[(i + len(p.name)) % len(KINDS)]
+                                                  for i in range(n)], dtype=object)
     if clip:
         first = [p.name for p in info.parameters.kernel_parameters
                  if p.polydisperse and p.type != "orientation"][0]
         cols[first + "_pd"][::13] = 0.5
         cols[first + "_pd_n"][::13] = 9
+    if magnetic:
+        for p in info.parameters.kernel_parameters:
+            if p.type == "sld":
+                m0 = rng.uniform(0, 3, n)
+                m0[::3] = 0.0
+                cols[p.name + "_M0"] = m0
+                cols[p.name + "_mtheta"] = rng.uniform(0, 180, n)
+                cols[p.name + "_mphi"] = rng.uniform(0, 360, n)
+        cols["up_frac_i"] = 0.9
+        cols["up_frac_f"] = 0.8
     cols["scale"] = 1.0
     return cols
 
@@ -54,14 +68,27 @@ def _row(cols, s):
     return out
 
 
-def _check_values(got, want, nvalues, length):
-    """Scalars and mesh points equal; weights within 2 ulp; zero padding."""
+def _check_values(got, want, nvalues, length, nmag=0, kinds=()):
+    """Scalars and mesh points equal; weights to the ulps exp/log/lgamma may
+    differ by (the schulz exponent z log z - ... cancels to ~1e-12 of its
+    terms); magnetic components to the ulps sin/cos may differ by; zero
+    padding."""
     a = nvalues + length
     b = nvalues + 2*length
+    m = nvalues - 3*nmag
     assert got.shape == want.shape
-    np.testing.assert_array_equal(got[:a], want[:a])
-    np.testing.assert_allclose(got[a:b], want[a:b], rtol=5e-16, atol=0)
+    np.testing.assert_array_equal(got[:m], want[:m])
+    np.testing.assert_allclose(got[m:nvalues], want[m:nvalues], rtol=2e-15,
+                               atol=2e-15*np.max(np.abs(want[m:nvalues]), initial=0.0))
+    np.testing.assert_array_equal(got[nvalues:a], want[nvalues:a])
+    wtol = 1e-11 if "schulz" in kinds else 4e-15
+    np.testing.assert_allclose(got[a:b], want[a:b], rtol=wtol, atol=0)
     np.testing.assert_array_equal(got[b:], want[b:])
+
+
+def _kinds(cols, s):
+    return [str(np.asarray(v)[s] if np.asarray(v).ndim else v)
+            for k, v in cols.items() if k.endswith("_pd_type")]
 
 
 def test_pairwise_sum_order_is_numpys():
@@ -81,25 +108,72 @@ def test_column_table_matches_make_call_args(name, dim):
     from sasmodels_b200.direct_model import make_call_args
     from sasmodels_b200.pack import column_args
     info = load_model_info(name)
-    n = 80
-    cols = _columns(info, n, 7)
+    n = 120
+    cols = _columns(info, n, 7, magnetic=dim == "2d")
     ca = column_args(info, n, cols, dim)
     vals = pack_ref.expand(ca)
     q = [np.zeros(1)] if dim == "1d" else [np.zeros(1), np.zeros(1)]
     off = 0
     assert ca["host_values"], "the population exercises the host path"
-    assert len(ca["host_values"]) < n
+    assert len(ca["host_values"]) < n//2       # one-point meshes go to the host
+    kinds_on_device = set()
     for s in range(n):
-        d0, v0, _ = make_call_args(info, _row(cols, s), q)
+        d0, v0, mag = make_call_args(info, _row(cols, s), q)
         np.testing.assert_array_equal(ca["det"][s], d0.buffer)
         assert ca["num_eval"][s] == d0.num_eval
         assert ca["val_sizes"][s] == v0.size
+        assert bool(ca["magnetic"][s]) == mag
         got = vals[off:off + v0.size]
         off += v0.size
         if s in ca["host_values"]:
             assert np.array_equal(got, v0)
         else:
-            _check_values(got, v0, info.parameters.nvalues, int(d0.num_weights))
+            kinds_on_device.update(pack_ref.KINDS[c] for c, m in zip(ca["kinds"][s],
+                                                                     ca["npts"][s]) if m > 0)
+            _check_values(got, v0, info.parameters.nvalues, int(d0.num_weights),
+                          info.parameters.nmagnetic if mag else 0, _kinds(cols, s))
+    assert kinds_on_device == set(pack_ref.KINDS)
+
+
+def _magnetic_population(n, seed=0):
+    """core_shell_sphere sets shaped like the magnetic headline: lognormal
+    radius (pd 0.2, 51 points), gaussian thickness (pd 0.1, 21 points), the
+    three slds' moments M0 ~ U[0,3], mtheta ~ U[0,180], mphi ~ U[0,360]."""
+    rng = np.random.default_rng(seed)
+    cols = dict(radius=rng.uniform(40, 80, n), radius_pd=0.2, radius_pd_n=51,
+                radius_pd_type="lognormal", thickness=rng.uniform(5, 15, n),
+                thickness_pd=0.1, thickness_pd_n=21, sld_core=1.0, sld_shell=2.0,
+                sld_solvent=3.0, up_frac_i=0.9, up_frac_f=0.8, up_theta=90.0, up_phi=45.0)
+    for sld in ("sld_core", "sld_shell", "sld_solvent"):
+        cols[sld + "_M0"] = rng.uniform(0, 3, n)
+        cols[sld + "_mtheta"] = rng.uniform(0, 180, n)
+        cols[sld + "_mphi"] = rng.uniform(0, 360, n)
+    return cols
+
+
+def test_magnetic_lognormal_population_packs_without_host():
+    """A population shaped like the magnetic headline is described entirely
+    by the device table: no set is marshaled by make_call_args, and the
+    restated expansion equals make_call_args's values."""
+    from sasmodels_b200.core import load_model_info
+    from sasmodels_b200.direct_model import make_call_args
+    from sasmodels_b200.pack import column_args
+    info = load_model_info("core_shell_sphere")
+    n = 24
+    cols = _magnetic_population(n)
+    ca = column_args(info, n, cols, "2d")
+    assert not ca["host_values"]
+    assert ca["magnetic"].all()
+    vals = pack_ref.expand(ca)
+    off = 0
+    q = [np.zeros(1), np.zeros(1)]
+    for s in range(n):
+        d0, v0, mag = make_call_args(info, _row(cols, s), q)
+        assert mag
+        np.testing.assert_array_equal(ca["det"][s], d0.buffer)
+        _check_values(vals[off:off + v0.size], v0, info.parameters.nvalues,
+                      int(d0.num_weights), info.parameters.nmagnetic, ["lognormal"])
+        off += v0.size
 
 
 def test_column_args_rejects_bad_columns():
@@ -177,6 +251,88 @@ def test_device_pack_matches_oracle_and_sets(cuda, model, line):
     ref.run()
     for a, b in zip(got, ref.iq()):
         np.testing.assert_allclose(a, b, rtol=1e-12, atol=0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("model", ["ellipsoid", "core_shell_cylinder"])
+def test_device_pack_every_distribution(cuda, model):
+    """Sets with every distribution of the plugin API and clipped meshes,
+    packed on the device: values against the restatement, and the batched
+    FP64 I(q) against the set-by-set (host-marshaled) population.  Schulz
+    weights differ from the host's by up to ~1e-12 (its exponent cancels),
+    so I(q) is held to 1e-11."""
+    from sasmodels_b200.batch import Population
+    from sasmodels_b200.core import load_model_info
+    info = load_model_info(model)
+    n = 90
+    cols = _columns(info, n, 17)
+    rng = np.random.default_rng(18)
+    qs = [np.geomspace(1e-3, 0.5, int(m)) for m in rng.integers(20, 200, n)]
+    pop = Population.from_columns(model, qs, cols, form="double")
+    assert len(pop.columns["host_values"]) < n//2
+    vals = pop.d_val.cpu().numpy()
+    want = pack_ref.expand(pop.columns)
+    off = 0
+    for s in range(n):
+        size = int(pop.columns["val_sizes"][s])
+        length = int(pop.columns["lengths"][s].sum())
+        if s in pop.columns["host_values"]:
+            assert np.array_equal(vals[off:off + size], want[off:off + size])
+        else:
+            _check_values(vals[off:off + size], want[off:off + size],
+                          info.parameters.nvalues, length, 0, _kinds(cols, s))
+        off += size
+    pop.run()
+    ref = Population(model, [(q, _row(cols, s)) for s, q in enumerate(qs)], form="double")
+    ref.run()
+    for a, b in zip(pop.iq(), ref.iq()):
+        np.testing.assert_allclose(a, b, rtol=1e-11, atol=0)
+
+
+@pytest.mark.gpu
+def test_device_pack_magnetic_drives_plain_kernel(cuda):
+    """Magnetic headline-shaped sets packed on the device (lognormal and
+    gaussian meshes, moments converted on the GPU) feed the plain Imagnetic
+    kernel straight from device memory: I(q) within 1e-12 of the same call
+    with host-marshaled values."""
+    import torch
+    from sasmodels_b200 import load_model
+    from sasmodels_b200.batch import _Packer
+    from sasmodels_b200.core import load_model_info
+    from sasmodels_b200.pack import column_args
+    from helpers import compare_raw, marshal
+    info = load_model_info("core_shell_sphere")
+    n = 6
+    cols = _magnetic_population(n, seed=3)
+    ca = column_args(info, n, cols, "2d")
+    assert not ca["host_values"]
+    model = load_model("core_shell_sphere")
+    x = np.linspace(-0.1, 0.1, 24)
+    qx, qy = [a.ravel() for a in np.meshgrid(x, x)]
+    kernel = model.make_kernel([qx, qy])
+    stream = kernel.stream
+    d_val = torch.empty(int(ca["val_sizes"].sum()), dtype=torch.float64, device=kernel.device)
+    packer = _Packer(ca, kernel.device, stream)
+    packer.load(ca)
+    packer.enqueue(d_val)
+    stream.synchronize()
+    off = 0
+    for s in range(n):
+        size = int(ca["val_sizes"][s])
+        details, values, magnetic = marshal(info, _row(cols, s), [qx, qy])
+        assert magnetic
+        dev_d, _ = kernel.upload(details, values)
+        nq = kernel.q_input.nq
+        with torch.cuda.stream(stream):
+            a = kernel.launch("Imagnetic", dev_d, d_val[off:off + size], 0,
+                              details.num_eval, 0.0, 0).clone()
+        kernel._call_kernel(details, values, 0.0, True, 0)
+        stream.synchronize()
+        b = kernel._result_dev.clone()
+        worst, f2rel = compare_raw(a.cpu().numpy()[:nq + 4], b.cpu().numpy()[:nq + 4],
+                                   1, nq, 1e-12)
+        assert worst <= 1.0, (s, worst, f2rel)
+        off += size
 
 
 @pytest.mark.gpu
