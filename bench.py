@@ -569,7 +569,8 @@ def run_b200(args, world, rank, local):
                                     "cpu": cpu_model()}
             line["parity_vs_dll"] = dict(errors_vs_dll(args.config, dev), sample=sample)
         if world == 1 and not args.no_extras and args.config == "cylinder2d":
-            line["extra"] = extras(dev, with_dll=not args.no_cpu, tile=tile or None)
+            line["extra"] = extras(dev, with_dll=not args.no_cpu, tile=tile or None,
+                                   surrogate=not args.no_surrogate)
         print(json.dumps(line), flush=True)
     return line
 
@@ -751,7 +752,7 @@ def smear_compare(dev, reps=50):
     return out
 
 
-def extras(dev, with_dll=True, tile=None):
+def extras(dev, with_dll=True, tile=None, surrogate=True):
     """Secondary measurements of the other headline configurations; with
     `with_dll`, each FP64 and FP32c form's max relative error against the
     reference DLL on that configuration's bounded CPU sample."""
@@ -787,7 +788,35 @@ def extras(dev, with_dll=True, tile=None):
     if with_dll:
         out["population"]["vs_dll"] = population_vs_dll(dev)
     out["smear_pinhole1d"] = smear_compare(dev)
+    if surrogate:
+        out["surrogate"] = surrogate_extra(dev)
     return out
+
+
+def surrogate_extra(dev, n_train_sets=50000, epochs=32, gate_epochs=16, n_holdout_sets=3000):
+    """The learned surrogate at its stated budget: 5e7 training samples
+    (50,000 sets x 1000 q), 32 epochs, the error gate on 1e7 fresh samples,
+    gate thresholds calibrated on 2000 held-out sets judged by the plain FP64
+    kernel and the measurement on the other 1000 held-out sets (1e6
+    samples): samples/s at 1 % log-I error with automatic fallback, against
+    the plain FP64 path on the same points."""
+    from sasmodels_b200.surrogate import train_and_evaluate
+    t0 = time.perf_counter()
+    _, rep = train_and_evaluate(n_train_sets=n_train_sets, nq=1000, epochs=epochs,
+                                gate_epochs=gate_epochs, n_holdout_sets=n_holdout_sets,
+                                device=dev)
+    op = rep["operating_points"]["0.01"]
+    return {"samples_per_s_at_1pct": op["samples_per_s"],
+            "speedup_vs_plain_f64": op["speedup"],
+            "speedup_vs_plain_f32c": op["speedup_vs_plain_f32c"],
+            "fallback_frac": op["fallback_frac"], "frac_within_1pct": op["frac_within"],
+            "max_log_err": op["max_err"], "heldout_samples": rep["holdout_samples"],
+            "net_only_median_err": rep["net_median_err"], "net_only_p99_err": rep["net_p99_err"],
+            "train_samples": rep["train_samples"], "epochs": rep["epochs"],
+            "data_s": rep["data_s"], "train_s": rep["train_s"], "gate_s": rep["gate_s"],
+            "wall_s": time.perf_counter() - t0,
+            "labels": "batched FP32c engine (within 1e-5 of FP64); judged by plain FP64",
+            "report": rep}
 
 
 def population_vs_dll(dev, stride=97, nq_sub=8, max_mesh=60000):
@@ -997,6 +1026,9 @@ def main(argv=None):
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the secondary configurations")
+    ap.add_argument("--no-surrogate", action="store_true",
+                    help="skip the surrogate's training and measurement in the extras "
+                         "(about four minutes)")
     args = ap.parse_args(argv)
     world, rank, local = dist_setup(args.gpus)
     try:

@@ -101,8 +101,11 @@ def test_tc_forward_matches_oracle(cuda):
     ref, _, _ = mlp_ref.forward(xh[:n], [mlp_ref.bf16(w) for w in W],
                                 [np.float32(v).astype(np.float64) for v in b],
                                 np.float32(w_out).astype(np.float64), np.float32(b_out))
+    # the oracle rounds every stored value as the kernel does; what remains
+    # is FP32 accumulation order and the fast exp/divide of SiLU, which move
+    # a rounding decision of the compensated activations now and then
     err = np.abs(got - ref).max()/np.abs(ref).max()
-    assert err < 2e-2, err
+    assert err < 2e-3, err
     # an FP64 forward without BF16 storage differs only at BF16 precision
     exact, _, _ = mlp_ref.forward(xh[:n], W, b, w_out, b_out, emulate_bf16=False)
     assert np.abs(got - exact).max()/np.abs(exact).max() < 5e-2
@@ -132,13 +135,13 @@ def test_tc_gradients_match_oracle(cuda):
         nb = 16 if l == 0 else 256
         g = dW[l].cpu().numpy().reshape(net.splits, 256, nb).sum(axis=0)
         rel = np.linalg.norm(g - rW[l])/np.linalg.norm(rW[l])
-        assert rel < 2e-2, (l, rel)
+        assert rel < 2e-3, (l, rel)
         rel = np.linalg.norm(db[l].cpu().numpy() - rb[l])/np.linalg.norm(rb[l])
-        assert rel < 2e-2, (l, "bias", rel)
+        assert rel < 2e-3, (l, "bias", rel)
     rel = np.linalg.norm(dwo.cpu().numpy() - rwo)/np.linalg.norm(rwo)
-    assert rel < 2e-2
+    assert rel < 2e-3
     assert abs(float(dbo.item()) - rbo) < 1e-3*max(1, abs(rbo))
-    assert abs(float(loss.item()) - np.mean((out[:n] - yv[:n])**2)) < 2e-2*np.mean((out[:n] - yv[:n])**2)
+    assert abs(float(loss.item()) - np.mean((out[:n] - yv[:n])**2)) < 2e-3*np.mean((out[:n] - yv[:n])**2)
 
 
 @pytest.mark.gpu
@@ -191,7 +194,7 @@ def test_tc_infer_matches_forward(cuda, n, blocks):
     ref, _, _ = mlp_ref.forward(xh[:min(n, 2000)], [mlp_ref.bf16(w) for w in W],
                                 [np.float32(v).astype(np.float64) for v in b],
                                 np.float32(w_out).astype(np.float64), np.float32(b_out))
-    assert np.abs(c[:len(ref)] - ref).max()/np.abs(ref).max() < 2e-2
+    assert np.abs(c[:len(ref)] - ref).max()/np.abs(ref).max() < 2e-3
 
 
 @pytest.mark.gpu
