@@ -775,6 +775,10 @@ def extras(dev, with_dll=True, tile=None, surrogate=True):
         v, t = single_config(name, qv, pars, dtype, 20, dev)
         out["magnetic_" + dtype] = {"evals_per_s": v, "ms_per_call": 1e3*t,
                                     "spin_channels": 6}
+    v, t = single_config(name, qv, pars, "double", 20, dev, form="plugin")
+    out["magnetic_plugin_f64"] = {
+        "evals_per_s": v, "ms_per_call": 1e3*t,
+        "what": "the plugin's Fq called once per spin channel, without the fused binding"}
     if with_dll:
         for config, keys in (("sphere1d", ("sphere1d_double", "sphere1d_float32c")),
                              ("cylinder2d", (None, "cylinder2d_float32c")),

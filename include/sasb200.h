@@ -126,6 +126,17 @@ int32_t sasb200_cylinder_Iqxy_noalloc(
     int32_t radius_effective_mode, int32_t tile, void *stream);
 
 SASB200_DECLARE_MODEL(core_shell_sphere)
+
+/*
+ * The core_shell_sphere library's sasb200_core_shell_sphere_Imagnetic
+ * evaluates the spin channels of a (q, mesh point) together: the two
+ * 3j1(x)/x terms and volumes of core_shell.c:8-30 once, then each channel's
+ * contrasts (kernel_iq.c:750-779 calls the model once per channel); within
+ * 1e-12 of the reference DLL.  The plugin's C as translated stays exported
+ * under the prefix core_shell_sphere_plugin (same arguments).
+ */
+SASB200_DECLARE_MODEL(core_shell_sphere_plugin)
+
 SASB200_DECLARE_MODEL(ellipsoid)
 SASB200_DECLARE_MODEL(core_shell_cylinder)
 

@@ -122,7 +122,8 @@ def build_model(name, force=False, verbose=False, extra_flags=()):
                               + _read(os.path.join(CSRC, "sas_abi.cuh"))
                               + _read(os.path.join(CSRC, "sas_device.cuh"))
                               + _read(os.path.join(CSRC, "sas_noalloc.cuh"))
-                              + _read(os.path.join(CSRC, "fp64_hoisted.cuh"))
+                              + "".join(_read(os.path.join(CSRC, h))
+                                        for h in generate.HOISTED_MODELS.values())
                               + _read(os.path.join(CSRC, "fp32c_math.cuh"))
                               + _read(os.path.join(CSRC, "fp32c_models.cuh"))
                               + _read(os.path.join(CSRC, "sas_batch.cuh")))

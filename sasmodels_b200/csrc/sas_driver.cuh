@@ -76,6 +76,33 @@ struct hoist_width<M, decltype((void)M::NH, void())> {
     static constexpr int value = M::NH;
 };
 
+// A binding may also evaluate all spin channels of the magnetic variant at
+// once (`MAG_FUSED`, `mag_channels(q, v, eff, chan_w)` for models without
+// orientation), sharing the channel-independent factors of its amplitude.
+template <class M, class = void>
+struct mag_fused { static constexpr bool value = false; };
+template <class M>
+struct mag_fused<M, decltype((void)M::MAG_FUSED, void())> {
+    static constexpr bool value = M::MAG_FUSED;
+};
+template <class M, bool ON>
+struct MagOps {
+    template <class E>
+    __device__ static double channels(double, const double *, const E &, const double *)
+    {
+        return 0.0;
+    }
+};
+template <class M>
+struct MagOps<M, true> {
+    template <class E>
+    __device__ static double channels(double q, const double *v, const E &eff,
+                                      const double *chan_w)
+    {
+        return M::mag_channels(q, v, eff, chan_w);
+    }
+};
+
 // Per-variant table layout.
 template <class M, int VAR>
 struct Layout {
@@ -490,13 +517,17 @@ __device__ __forceinline__ void accumulate_rows(const QState<M, VAR> &qs,
             } else if constexpr (QState<M, VAR>::MAG) {
                 double F2 = 0.0;
                 if (qs.mag_on) {
-                    #pragma unroll
-                    for (int c = 0; c < 5; ++c) {
-                        if (qs.chan_w[c] > 0.0) {
-                            #pragma unroll
-                            for (int sk = 0; sk < M::NMAG; ++sk)
-                                v[M::mag_par(sk)] = qs.eff[c][sk];
-                            F2 += qs.chan_w[c]*eval_2d<M, XY>(qs.qx, qs.qy, qs.qk, rot, v);
+                    if constexpr (mag_fused<M>::value && XY == XY_QA) {
+                        F2 = MagOps<M, true>::channels(qs.qk, v, qs.eff, qs.chan_w);
+                    } else {
+                        #pragma unroll
+                        for (int c = 0; c < 5; ++c) {
+                            if (qs.chan_w[c] > 0.0) {
+                                #pragma unroll
+                                for (int sk = 0; sk < M::NMAG; ++sk)
+                                    v[M::mag_par(sk)] = qs.eff[c][sk];
+                                F2 += qs.chan_w[c]*eval_2d<M, XY>(qs.qx, qs.qy, qs.qk, rot, v);
+                            }
                         }
                     }
                 }

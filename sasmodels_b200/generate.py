@@ -37,11 +37,14 @@ XY_CODES = {"qa": 1, "qac": 2, "qabc": 3, "qxy": 4}
 #: sasb200_<model>_<variant>_noalloc (csrc/sas_noalloc.cuh)
 NOALLOC_EXPORTS = {"cylinder": ("Iqxy", "sasb200::VAR_IQXY")}
 
-#: models with a hand-rearranged FP64 binding that hoists per-mesh-point work
-#: out of the q loop of one 2D form (header in csrc/, struct SasModelHoisted).
-#: Their library's sasb200_<model>_* entry points use it; the plugin's C as
-#: translated stays exported as sasb200_<model>_plugin_* for comparison.
-HOISTED_MODELS = {"cylinder": "fp64_hoisted.cuh"}
+#: models with a hand-rearranged FP64 binding (header in csrc/, struct
+#: SasModelHoisted): cylinder hoists per-mesh-point work out of the q loop of
+#: its 2D form; core_shell_sphere evaluates the spin channels of its magnetic
+#: form together.  Their library's sasb200_<model>_* entry points use it; the
+#: plugin's C as translated stays exported as sasb200_<model>_plugin_* for
+#: comparison.
+HOISTED_MODELS = {"cylinder": "fp64_hoisted_cylinder.cuh",
+                  "core_shell_sphere": "fp64_hoisted_core_shell_sphere.cuh"}
 
 _IQXY_RE = re.compile(r"(^|\s)double\s+I(?P<mode>q(ac|abc|xy))\s*[(]", re.M)
 _SHELL_RE = re.compile(r"(^|\s)double\s+shell_volume\s*[(]", re.M)

@@ -333,3 +333,32 @@ def test_hoisted_cylinder_matches_plugin_form(cuda):
     worst, f2rel = compare_raw(fast.cpu().numpy()[:nq + 4], out.cpu().numpy(), 1, nq, 1e-12)
     assert worst <= 1.0, (worst, f2rel)
     assert_parity(name, qv, pars)
+
+
+def test_fused_magnetic_matches_plugin_form(cuda):
+    """core_shell_sphere Imagnetic with the spin channels sharing one
+    evaluation of the Bessel terms against the plugin's C called per
+    channel (sasb200_core_shell_sphere_plugin_Imagnetic), on the magnetic
+    headline's grid at a reduced mesh; and against the DLL."""
+    import torch
+    from sasmodels_b200 import _abi
+    name, qv, pars = workloads.core_shell_sphere_magnetic(n=48, radius_n=9, thickness_n=5)
+    model = load_model(name)
+    kernel = model.make_kernel(qv)
+    details, values, magnetic = marshal(model.info, pars, qv)
+    assert magnetic
+    dev_d, dev_v = kernel.upload(details, values)
+    plugin = _abi.load_library(name, form="plugin")
+    nq, n = kernel.q_input.nq, details.num_eval
+    out = torch.zeros(nq + 4, dtype=torch.float64, device=kernel.device)
+    with torch.cuda.stream(kernel.stream):
+        fused = kernel.launch("Imagnetic", dev_d, dev_v, 0, n, 0.0, 0).clone()
+        ws = torch.empty(max(plugin.workspace_bytes("Imagnetic", nq, n, 0), 256),
+                         dtype=torch.uint8, device=kernel.device)
+        plugin.call("Imagnetic", nq, 0, n, dev_d.data_ptr(), dev_v.data_ptr(),
+                    kernel.q_input.q_dev.data_ptr(), out.data_ptr(), 0.0, 0,
+                    ws.data_ptr(), ws.numel(), 0, kernel.stream.cuda_stream)
+    kernel.stream.synchronize()
+    worst, f2rel = compare_raw(fused.cpu().numpy()[:nq + 4], out.cpu().numpy(), 1, nq, 1e-12)
+    assert worst <= 1.0, (worst, f2rel)
+    assert_parity(name, qv, pars)
