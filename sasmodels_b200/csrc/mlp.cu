@@ -753,30 +753,38 @@ mlp_infer(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
                 tc::fence_after_sync();
                 ok = tc::bar_and(1, INF_CONSUMERS, ok && done);
                 if (!ok) break;
-                // epilogue: this thread's row, columns [128 half, 128 half + 128)
+                // epilogue: this thread's row, columns [128 half, 128 half + 128),
+                // 32 columns per TMEM wait (two loads in flight), each group of
+                // 16 processed in column order as before
                 const float *bias = prm.b[l];
                 float dot = 0.0f;
                 #pragma unroll 1
-                for (int c0 = 128*half; c0 < 128*half + 128; c0 += 16) {
-                    uint32_t r16[16];
-                    tc::tmem_ld16(tmem + lane_base + (uint32_t)c0, r16);
+                for (int c32 = 128*half; c32 < 128*half + 128; c32 += 32) {
+                    uint32_t r32[2][16];
+                    tc::tmem_ld16(tmem + lane_base + (uint32_t)c32, r32[0]);
+                    tc::tmem_ld16(tmem + lane_base + (uint32_t)(c32 + 16), r32[1]);
                     tc::tmem_wait_ld();
-                    float z[16], h[16];
                     #pragma unroll
-                    for (int j = 0; j < 16; ++j) {
-                        z[j] = __uint_as_float(r16[j]) + bias[c0 + j];
-                        h[j] = silu(z[j]);
-                    }
-                    if (prm.z_save != nullptr) {
-                        const size_t at = (size_t)l*plane + (size_t)(row0 + row)*HID + c0;
-                        save16(prm.z_save + at, z);
-                        save16(prm.h_save + at, h);
-                    }
-                    if (l == 3) {
+                    for (int g = 0; g < 2; ++g) {
+                        const int c0 = c32 + 16*g;
+                        float z[16], h[16];
                         #pragma unroll
-                        for (int j = 0; j < 16; ++j) dot = fmaf(h[j], prm.w_out[c0 + j], dot);
-                    } else {
-                        store16_split(act, act_lo, row, c0, h);
+                        for (int j = 0; j < 16; ++j) {
+                            z[j] = __uint_as_float(r32[g][j]) + bias[c0 + j];
+                            h[j] = silu(z[j]);
+                        }
+                        if (prm.z_save != nullptr) {
+                            const size_t at = (size_t)l*plane + (size_t)(row0 + row)*HID + c0;
+                            save16(prm.z_save + at, z);
+                            save16(prm.h_save + at, h);
+                        }
+                        if (l == 3) {
+                            #pragma unroll
+                            for (int j = 0; j < 16; ++j)
+                                dot = fmaf(h[j], prm.w_out[c0 + j], dot);
+                        } else {
+                            store16_split(act, act_lo, row, c0, h);
+                        }
                     }
                 }
                 if (l == 3) {
