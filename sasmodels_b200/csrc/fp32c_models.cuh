@@ -98,6 +98,37 @@ struct QuadCoreShellSphere {
     }
 };
 
+// The magnetic form of core_shell_sphere with its spin channels sharing one
+// evaluation of the two Bessel terms (QuadCoreShellSphere's arithmetic, the
+// channel's effective slds in place of v[2..4]): sum over the channels c
+// with chan_w[c] > 0 of chan_w[c] * F^2.  mag_par(k) gives the slot of
+// magnetic sld k in v.
+template <class MagPar>
+__device__ __forceinline__ double core_shell_sphere_channels(double q, const double *v,
+                                                             const double (*eff)[3],
+                                                             const double *chan_w, MagPar mag_par)
+{
+    const double rt = v[0] + v[1];
+    const float bc = sph_j1c_f(q*v[0]);
+    const float bs = sph_j1c_f(q*rt);
+    const double vc = FOUR_PI_3*v[0]*v[0]*v[0];
+    const double vs = FOUR_PI_3*rt*rt*rt;
+    double F2 = 0.0;
+    #pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        if (chan_w[c] > 0.0) {
+            double sl[5] = {v[0], v[1], v[2], v[3], v[4]};
+            #pragma unroll
+            for (int k = 0; k < 3; ++k) sl[mag_par(k)] = eff[c][k];
+            const float core = (float)(vc*(sl[2] - sl[3]));
+            const float shell = (float)(vs*(sl[3] - sl[4]));
+            const double f = (double)(core*bc + shell*bs);
+            F2 += chan_w[c]*(1.0e-4*fma(f, f, 0.0));
+        }
+    }
+    return F2;
+}
+
 // cylinder (cylinder.c:55-88): v = sld, sld_solvent, radius, length, ...
 struct QuadCylinder {
     struct S { double qr, qh, s; Rule r; };

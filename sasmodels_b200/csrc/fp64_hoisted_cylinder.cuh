@@ -14,17 +14,20 @@
 // Arithmetic is rearranged, not approximated differently:
 //
 //   * mesh_prepare stores per kept mesh point the row
-//       [ w * 1e-4 * (drho pi R^2 L)^2,  R,  L/2,  R31,  R32,  0 ]
+//       [ w * 1e-4 * (drho pi R^2 L)^2,  R,  L/2,  R31,  R32,  R^2 ]
 //     so the contrast, volume, scale factor and weight product are formed
 //     once per point instead of once per (q, point);
 //   * |q|^2 is formed once per q, and qab^2 = |q|^2 - qc^2;
-//   * 2 J1(x)/x on x <= 5 is 2 P(z)/Q(z) (z - Z1)(z - Z2): the reference's
-//     J1 = x P/Q (z - Z1)(z - Z2) with the factor x cancelled against the
-//     division by x;
+//   * 2 J1(x)/x on x <= 5 is 2 P(z)/Q(z) (z - Z1)(z - Z2) with z = x^2 =
+//     qab^2 R^2: the reference's J1 = x P/Q (z - Z1)(z - Z2) with the
+//     factor x cancelled against the division by x, and no square root for
+//     qab on this branch (about four evaluations in five);
 //   * on x > 5 the two polynomial ratios share one division, 5/x and the
 //     final 1/x share one reciprocal, and 1/sqrt(x) is a reciprocal square
-//     root: three divisions and a square root of the reference become two
-//     divisions and a reciprocal square root.
+//     root;
+//   * sin(y)/y of the length factor joins the J1 term's division, so an
+//     evaluation divides once on x <= 5 and twice on x > 5 (the reference:
+//     three and five times).
 //
 // Each change moves a result by a few units in the last place; the mesh
 // sums of these non-negative terms stay within 1e-12 of the reference DLL
@@ -49,39 +52,67 @@ struct SasModelHoisted : SasModel {
         row[2] = 0.5*v[3];
         row[3] = rot[0];
         row[4] = rot[1];
-        row[5] = 0.0;
+        row[5] = v[2]*v[2];
     }
 
-    // 2 J1(x)/x for x = qab R >= 0
-    __device__ static double j1x(double x)
+    // two consecutive doubles of a 16-byte aligned row in one shared load
+    __device__ static void pair(const double *p, double &a, double &b)
     {
-        const double ax = fabs(x);
-        if (ax <= 5.0) {
-            const double z = ax*ax;
-            const double r = polevl(z, RPJ1, 3)/p1evl(z, RQJ1, 8);
-            return 2.0*r*(z - Z1)*(z - Z2);
+#ifdef __CUDA_ARCH__
+        const double2 t = *reinterpret_cast<const double2 *>(p);
+        a = t.x;
+        b = t.y;
+#else
+        a = p[0];
+        b = p[1];
+#endif
+    }
+
+    // 2 J1(x)/x as num/den, for x^2 = z (x = qab R >= 0; qab_sq = qab^2)
+    __device__ static void j1x_parts(double z, double qab_sq, double R, double &num,
+                                     double &den)
+    {
+        if (z <= 25.0) {
+            num = 2.0*polevl(z, RPJ1, 3)*(z - Z1)*(z - Z2);
+            den = p1evl(z, RQJ1, 8);
+            return;
         }
+        const double ax = sqrt(qab_sq)*R;
         const double inv = 1.0/ax;
         const double w = 5.0*inv;
-        const double z = w*w;
-        const double pp = polevl(z, PPJ1, 6), pq = polevl(z, PQJ1, 6);
-        const double qp = polevl(z, QPJ1, 7), qq = p1evl(z, QQJ1, 7);
+        const double zz = w*w;
+        const double pp = polevl(zz, PPJ1, 6), pq = polevl(zz, PQJ1, 6);
+        const double qp = polevl(zz, QPJ1, 7), qq = p1evl(zz, QQJ1, 7);
         double sn, cs;
         sincos(ax, &sn, &cs);
         // p (sin - cos) + w q (sin + cos), p = pp/pq, q = qp/qq
-        const double num = pp*qq*(sn - cs) + w*qp*pq*(sn + cs);
-        return (2.0*SQRT1_PI)*(num/(pq*qq))*inv*rsqrt(ax);
+        num = (pp*qq*(sn - cs) + w*qp*pq*(sn + cs))*((2.0*SQRT1_PI)*inv*rsqrt(ax));
+        den = pq*qq;
+    }
+
+    // 2 J1(x)/x for x >= 0 (used by the host checks)
+    __device__ static double j1x(double x)
+    {
+        double num, den;
+        j1x_parts(x*x, x*x, 1.0, num, den);
+        return num/den;
     }
 
     __device__ static double eval_row(double qx, double qy, double qsq, const double *row)
     {
-        const double qc = row[3]*qx + row[4]*qy;
+        double A, R, halfL, R31, R32, R2;
+        pair(row, A, R);
+        pair(row + 2, halfL, R31);
+        pair(row + 4, R32, R2);
+        const double qc = R31*qx + R32*qy;
         const double qab_sq = qsq - qc*qc;
-        const double qab = qab_sq > 0.0 ? sqrt(qab_sq) : 0.0;
-        const double bes = j1x(qab*row[1]);
-        const double y = qc*row[2];
-        const double sn = y == 0.0 ? 1.0 : sin(y)/y;
-        const double f = bes*sn;
-        return row[0]*(f*f);
+        const double z = qab_sq > 0.0 ? qab_sq*R2 : 0.0;
+        double num, den;
+        j1x_parts(z, qab_sq, R, num, den);
+        // sin(y)/y folded into the same division (1 at y = 0)
+        const double y = qc*halfL;
+        const bool y0 = y == 0.0;
+        const double f = (num*(y0 ? 1.0 : sin(y)))/(den*(y0 ? 1.0 : y));
+        return A*(f*f);
     }
 };

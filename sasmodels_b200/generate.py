@@ -491,6 +491,13 @@ def f32c_block(name, table, codes):
     out.append("  __device__ static double iq(double q, const double *v) { double F1, F2; fq(q, F1, F2, v); return F2; }")
     if iqac:
         out.append("  __device__ static double iqac(double qab, double qc, const double *v) { %s }" % iqac)
+    if name == "core_shell_sphere":
+        # the spin channels of the magnetic form share the Bessel terms
+        out.append("  static constexpr bool MAG_FUSED = true;")
+        out.append("  __device__ static double mag_channels(double q, const double *v,"
+                   " const double (*eff)[3], const double *chan_w)"
+                   " { return f32c::core_shell_sphere_channels(q, v, eff, chan_w,"
+                   " [](int k) { return mag_par(k); }); }")
     out.append("};")
     out.append("}  // namespace sasm")
     return "\n".join(out)
