@@ -576,6 +576,9 @@ def run_b200(args, world, rank, local):
 
 
 def time_launches(kernel, variant, dd, dv, n_mesh, reps):
+    """Seconds per call of `reps` back-to-back launches on the kernel's
+    stream, CUDA events around them (host launch overhead included when it
+    exceeds the device time of a call)."""
     import torch
     stream = kernel.stream
     with torch.cuda.stream(stream):
@@ -587,6 +590,30 @@ def time_launches(kernel, variant, dd, dv, n_mesh, reps):
             kernel.launch(variant, dd, dv, 0, n_mesh, 0.0, 0)
         stop.record(stream)
     stop.synchronize()
+    return start.elapsed_time(stop)*1e-3/reps
+
+
+def time_graph(kernel, variant, dd, dv, n_mesh, reps):
+    """Device seconds per call: `reps` launches captured in one CUDA graph and
+    replayed, CUDA events around the replay (no host work between calls)."""
+    import torch
+    stream = kernel.stream
+    with torch.cuda.stream(stream):
+        kernel.launch(variant, dd, dv, 0, n_mesh, 0.0, 0)      # workspace, tile, module
+    stream.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        for _ in range(reps):
+            kernel.launch(variant, dd, dv, 0, n_mesh, 0.0, 0)
+    with torch.cuda.stream(stream):
+        graph.replay()
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        graph.replay()
+        stop.record(stream)
+    stop.synchronize()
+    del graph
     return start.elapsed_time(stop)*1e-3/reps
 
 
@@ -605,6 +632,26 @@ def single_config(name, qv, pars, dtype, reps, dev, form=None, tile=None):
     dd, dv = kernel.upload(details, values)
     t = time_launches(kernel, kernel.variant(magnetic), dd, dv, details.num_eval, reps)
     return len(qv[0])*details.num_eval/t, t
+
+
+def small_config(name, qv, pars, dtype, reps, dev):
+    """evals/s of a call shape whose device time is below the host's launch
+    overhead: device time per call from a CUDA graph of `reps` launches, and
+    the host-launched loop beside it."""
+    from sasmodels_b200 import load_model
+    model = load_model(name, dtype=dtype, device=dev)
+    kernel = model.make_kernel(qv)
+    details, values, magnetic = marshal(model.info, pars, qv)
+    dd, dv = kernel.upload(details, values)
+    variant = kernel.variant(magnetic)
+    t_graph = time_graph(kernel, variant, dd, dv, details.num_eval, reps)
+    t_loop = time_launches(kernel, variant, dd, dv, details.num_eval, reps)
+    evals = len(qv[0])*details.num_eval
+    return {"evals_per_s": evals/t_graph, "ms_per_call": 1e3*t_graph,
+            "timing": "device time per call, %d calls replayed from one CUDA graph" % reps,
+            "launches_per_call": kernel.lib.launches(variant, kernel.q_input.nq,
+                                                     details.num_eval),
+            "host_loop_evals_per_s": evals/t_loop, "host_loop_ms_per_call": 1e3*t_loop}
 
 
 def population_compare(n_sets, stride, dev, tune=True):
@@ -768,8 +815,7 @@ def extras(dev, with_dll=True, tile=None, surrogate=True):
     out = {}
     name, qv, pars = workloads.sphere_1d()
     for dtype in ("double", "float32c"):
-        v, t = single_config(name, qv, pars, dtype, 200, dev)
-        out["sphere1d_" + dtype] = {"evals_per_s": v, "ms_per_call": 1e3*t}
+        out["sphere1d_" + dtype] = small_config(name, qv, pars, dtype, 200, dev)
     name, qv, pars = workloads.cylinder_2d()
     v, t = single_config(name, qv, pars, "float32c", 3, dev)
     out["cylinder2d_float32c"] = {"evals_per_s": v, "ms_per_call": 1e3*t}
