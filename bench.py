@@ -496,7 +496,9 @@ def run_b200(args, world, rank, local):
             barrier()
             te = dist_max(time.perf_counter() - t0)
         e2e = {"value": evals_all*args.steps/te, "unit": UNIT,
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "breakdown_ms": e2e_breakdown(model, qhost, details, values, magnetic,
+                                             variant, n_mesh)}
         s = e2e_clocks.summary()
         if s:
             e2e["clocks"] = s
@@ -573,6 +575,41 @@ def run_b200(args, world, rank, local):
                                    surrogate=not args.no_surrogate)
         print(json.dumps(line), flush=True)
     return line
+
+
+def e2e_breakdown(model, qhost, details, values, magnetic, variant, n_mesh):
+    """Where one end-to-end step's time goes (host clock, synchronised
+    between phases): make_kernel (q ordering and upload, buffers), the call
+    (values upload, kernels, I(q) back and normalised) with the kernels'
+    own device time from CUDA events, and release; plus the tile the call
+    ran on."""
+    import torch
+    from sasmodels_b200 import autotune
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    k = model.make_kernel(qhost)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    k(details, values, 0.0, magnetic)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    dd, dv = k.upload(details, values)
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(k.stream):
+        start.record(k.stream)
+        k.launch(variant, dd, dv, 0, n_mesh, 0.0, 0)
+        stop.record(k.stream)
+    stop.synchronize()
+    tile = autotune.cached_tile(k, variant, n_mesh)
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
+    k.release()
+    torch.cuda.synchronize()
+    t4 = time.perf_counter()
+    return {"make_kernel": 1e3*(t1 - t0), "call": 1e3*(t2 - t1),
+            "kernels_device": start.elapsed_time(stop), "release": 1e3*(t4 - t3),
+            "tile": "0x%08x" % tile}
 
 
 def time_launches(kernel, variant, dd, dv, n_mesh, reps):
@@ -929,16 +966,17 @@ SASFLOPS = {
 #: per thread instruction) over the evaluations of the captured launch; the
 #: issued count includes the operations CUDA's sin, sqrt and division expand
 #: into, so it sits above the algorithmic count (profiles/iq_main_*.md).
-ISSUED_FP64_PER_EVAL = {"magnetic": 758.0}
+ISSUED_FP64_PER_EVAL = {"cylinder2d": 101.6}
 #: XU-pipe (MUFU sin/cos/rcp/rsqrt and conversions) thread operations per
 #: evaluation of the FP32c form of iq_main: ncu's sm__inst_executed_pipe_xu
 #: (51.6 % of a 16-lane-per-clock peak over the elapsed cycles) x 32 lanes
 #: / evaluations of the captured launch (profiles/iq_main_cylinder2d_f32c.md)
 XU_OPS_PER_EVAL = {"cylinder2d": 12.3}
-#: dram read+write bytes of the dominant kernel per launch (ncu): the mesh
-#: table is read once from DRAM and then served from L2; it does not grow
-#: with the number of q points (profiles/iq_main_cylinder2d.md)
-TRAFFIC_PER_STEP = {"cylinder2d": 40.83e6}
+#: dram read+write bytes of the dominant kernel per launch (ncu, on the
+#: 64x64-q case of the same mesh): the 490,000 hoisted 48-byte rows of the
+#: mesh table are read once from DRAM and then served from L2, so the figure
+#: does not grow with the number of q points (profiles/iq_main_cylinder2d.md)
+TRAFFIC_PER_STEP = {"cylinder2d": 23.62e6}
 
 
 def run_population(args, world, rank, local):
