@@ -169,6 +169,11 @@ def gpu_selector(local_device):
 
 
 def dist_setup(n_gpus):
+    """(world, rank, device index) from the torchrun environment; one
+    process per GPU over NCCL.  SASB200_BENCH_BACKEND=gloo runs the
+    collectives on the host instead, with ranks placed round-robin on the
+    visible GPUs: a check of the multi-rank logic on a box with fewer GPUs
+    than ranks (its timings mean nothing; no kernel waits on another rank)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -176,9 +181,15 @@ def dist_setup(n_gpus):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        backend = os.environ.get("SASB200_BENCH_BACKEND", "nccl")
+        if backend == "gloo":
+            local = local % max(torch.cuda.device_count(), 1)
+            torch.cuda.set_device(local)
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+        else:
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
     return world, rank, local
 
 
@@ -187,7 +198,8 @@ def dist_max(x):
     import torch.distributed as dist
     if not (dist.is_available() and dist.is_initialized()):
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
