@@ -84,8 +84,8 @@ extern "C" {
      * larger ranges take three launches per workspace chunk; no reference \
      * counterpart */ \
     int32_t sasb200_##M##_single_launch_max(int32_t variant); \
-    /* tile code the library picks for (nq, n_mesh) when tile == 0 */ \
-    int32_t sasb200_##M##_default_tile(int32_t nq, int32_t n_mesh); \
+    /* tile code the library picks for (variant, nq, n_mesh) when tile == 0 */ \
+    int32_t sasb200_##M##_default_tile(int32_t variant, int32_t nq, int32_t n_mesh); \
     /* message of the last failed call on this host thread ("" if none) */ \
     const char *sasb200_##M##_last_error(void);
 

@@ -72,7 +72,7 @@ class ModelLib:
         self._ntile = self._fn("tile_count", ct.c_int32, [])
         self._tile = self._fn("tile_code", ct.c_int32, [ct.c_int32])
         self._default_tile = self._fn("default_tile", ct.c_int32,
-                                      [ct.c_int32, ct.c_int32])
+                                      [ct.c_int32, ct.c_int32, ct.c_int32])
         self._single_max = self._fn("single_launch_max", ct.c_int32, [ct.c_int32])
 
     def _fn(self, suffix, restype, argtypes):
@@ -91,8 +91,8 @@ class ModelLib:
     def tile_shapes(self):
         return [int(self._tile(i)) for i in range(int(self._ntile()))]
 
-    def default_tile(self, nq, n_mesh):
-        return int(self._default_tile(nq, n_mesh))
+    def default_tile(self, variant, nq, n_mesh):
+        return int(self._default_tile(VARIANT_ID[variant], nq, n_mesh))
 
     def single_launch_max(self, variant):
         """Largest mesh range the library evaluates in one kernel launch."""

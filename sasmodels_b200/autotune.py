@@ -98,8 +98,8 @@ def tile_candidates(lib, nq, n_mesh, sms=148):
     for code in lib.tile_shapes():
         lq, warps = code & 0xff, (code >> 8) & 0xff
         qtiles = max(1, (nq + lq - 1)//lq)
-        for blocks_per_sm in (8, 32, 64, 128):
-            splits = int(min(nseg, max(1, np.ceil(sms*blocks_per_sm/qtiles)), 4096))
+        for blocks_per_sm in (8, 32, 128, 512):
+            splits = int(min(nseg, max(1, np.ceil(sms*blocks_per_sm/qtiles)), 128))
             out.append((splits << 16) | (warps << 8) | lq)
     return sorted(set(out))
 

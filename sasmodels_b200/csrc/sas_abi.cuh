@@ -71,24 +71,30 @@ __host__ inline int device_sms()
     return cached_sms;
 }
 
-// Built-in tile choice: wide q tiles when there are many q points, mesh
-// lanes when there are few, then enough mesh splits to give every SM several
-// blocks.
-__host__ inline Tile choose_tile(int nq, int n_mesh)
+// Built-in tile choice, fitted to timings of the current kernels on B200
+// (cylinder 2D at 4,096 and 65,536 q x 490,000 points, the magnetic
+// core_shell_sphere, a 1D ellipsoid with adaptive quadrature):
+//   * 1D calls: one q per warp (the 32 lanes take mesh points), 4 warps --
+//     every lane of a warp then runs the same quadrature rule (2.3x the
+//     8-q tile for the ellipsoid);
+//   * 2D calls: 32 neighbouring q per warp from 16,384 q up, 8 below, mesh
+//     lanes under 256 q, 4 warps;
+//   * then mesh splits for ~512 blocks per SM (at most 128 splits, at most
+//     one per 128-point segment): cylinder 2D runs 5 % faster at 32-64
+//     splits than at 5.
+__host__ inline Tile choose_tile(int nq, int n_mesh, bool one_d)
 {
     Tile t;
-    if (nq >= 4096) t = Tile{32, 4, 1};
+    if (one_d) t = Tile{1, 4, 1};
+    else if (nq >= 16384) t = Tile{32, 4, 1};
     else if (nq >= 256) t = Tile{8, 4, 1};
     else t = Tile{1, 8, 1};
     const long long qtiles = (nq + t.lq - 1)/t.lq;
     const long long nseg = (n_mesh + SEG - 1)/SEG;
-    // ~64 blocks per SM: enough blocks that the last wave is a small
-    // fraction of the launch (measured on cylinder 2D: 8 splits of 2048 q
-    // tiles run 8% faster than 2)
-    const long long want = (long long)device_sms()*64;
+    const long long want = (long long)device_sms()*512;
     long long splits = qtiles > 0 ? (want + qtiles - 1)/qtiles : 1;
     if (splits > nseg) splits = nseg;
-    if (splits > 4096) splits = 4096;
+    if (splits > 128) splits = 128;
     if (splits < 1) splits = 1;
     t.splits = (int)splits;
     return t;
@@ -188,7 +194,8 @@ template <class M, int VAR>
 __host__ uint64_t workspace_bytes(int32_t nq, int32_t n_mesh, int32_t tile_code)
 {
     if (nq < 0 || n_mesh < 0) return 0;
-    Tile t = tile_code ? tile_decode(tile_code) : choose_tile(nq, n_mesh);
+    Tile t = tile_code ? tile_decode(tile_code)
+                       : choose_tile(nq, n_mesh, Layout<M, VAR>::XY == XY_1D);
     // at least one segment, at most 2^20 mesh points per pass
     const long long chunk = n_mesh < 1 ? 1 : (n_mesh < (1 << 20) ? n_mesh : (1 << 20));
     return Workspace<M, VAR>(nq, chunk, t.splits).total;
@@ -214,7 +221,8 @@ __host__ int32_t run(int32_t nq, int32_t pd_start, int32_t pd_stop,
     if (!details || !values || !result || (nq > 0 && !q))
         return fail(ERR_ARGUMENT, "null array pointer");
     const int n_mesh = pd_stop - pd_start;
-    Tile t = tile_code ? tile_decode(tile_code) : choose_tile(nq, n_mesh);
+    Tile t = tile_code ? tile_decode(tile_code)
+                       : choose_tile(nq, n_mesh, Layout<M, VAR>::XY == XY_1D);
     if (!shape_ok(t) || t.splits < 1)
         return fail(ERR_ARGUMENT, "unknown tile code");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -348,9 +356,10 @@ extern "C" int32_t sasb200_##NAME##_tile_code(int32_t i)                        
     if (i < 0 || i >= sasb200::N_SHAPES) return 0;                                      \
     return sasb200::tile_encode(sasb200::shape_at(i));                                  \
 }                                                                                       \
-extern "C" int32_t sasb200_##NAME##_default_tile(int32_t nq, int32_t n_mesh)            \
+extern "C" int32_t sasb200_##NAME##_default_tile(int32_t variant, int32_t nq,          \
+                                                  int32_t n_mesh)                       \
 {                                                                                       \
-    return sasb200::tile_encode(sasb200::choose_tile(nq, n_mesh));                       \
+    return sasb200::tile_encode(sasb200::choose_tile(nq, n_mesh, variant == 0));         \
 }                                                                                       \
 extern "C" const char *sasb200_##NAME##_last_error(void)                                \
 {                                                                                       \

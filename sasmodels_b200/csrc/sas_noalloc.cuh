@@ -69,7 +69,9 @@ __host__ int32_t run_static(int32_t nq, int32_t pd_start, int32_t pd_stop,
 {
     if (nq < 0 || pd_start < 0 || pd_stop < pd_start)
         return fail(ERR_ARGUMENT, "need nq >= 0 and 0 <= pd_start <= pd_stop");
-    const Tile t = tile_code ? tile_decode(tile_code) : choose_tile(nq, pd_stop - pd_start);
+    const Tile t = tile_code ? tile_decode(tile_code)
+                             : choose_tile(nq, pd_stop - pd_start,
+                                           Layout<M, VAR>::XY == XY_1D);
     if (!shape_ok(t) || t.splits < 1)
         return fail(ERR_ARGUMENT, "unknown tile code");
     const size_t need = Workspace<M, VAR>(nq, SEG, t.splits).total;

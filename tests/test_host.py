@@ -157,8 +157,12 @@ def test_abi_host_queries(name):
     n = lib.workspace_bytes("Iq", 1000, 35)
     assert n >= 35*8 and n % 256 == 0
     assert lib.workspace_bytes("Iqxy", 65536, 490000, 0) > 490000*8
-    tile = lib.default_tile(1000, 35)
+    tile = lib.default_tile("Iqxy", 1000, 35)
     assert (tile & 0xff) in (1, 8, 32)
+    # 1D: one q per warp; large 2D: 32 neighbouring q per warp, many splits
+    assert lib.default_tile("Iq", 1000, 1225) & 0xff == 1
+    big = lib.default_tile("Iqxy", 65536, 490000)
+    assert big & 0xff == 32 and 16 <= (big >> 16) <= 128
 
 
 def test_abi_rejects_bad_arguments_without_gpu():
