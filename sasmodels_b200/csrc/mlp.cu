@@ -806,6 +806,298 @@ mlp_infer(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
     if (warp == 0) tc::tmem_dealloc(tmem, HID);
 }
 
+// ------------------------------------------------------------------ serve --
+// mlp_serve: inference only (no z/h planes), with the tensor core and the
+// epilogue busy at the same time.  Arithmetic per element as mlp_infer
+// (bias, SiLU, the compensated hi/lo split rounded to nearest), so the
+// hidden activations are bitwise those of mlp_infer; the output dot sums
+// the 256 columns in another order (four partial sums per row).
+//
+// Roles, 18 warps per CTA (one CTA per SM, persistent over 128-row tiles):
+//   warps 0-15  epilogue.  Warp w reads the TMEM lanes of its quadrant
+//               (rows 32(w%4) .. +31) and, of every 32-column chunk, the 8
+//               columns at 8(w/4).  Chunk by chunk: bias + SiLU + split into
+//               the activation tile, then one arrive per warp on
+//               act_ready[chunk].
+//   warp 16     lane 0 issues every MMA; all lanes load the next tile's
+//               features while the tensor core runs the last layer.
+//   warp 17     the bulk-copy producer of the weight ring (as mlp_infer).
+// Two TMEM accumulators (columns [0, 256) and [256, 512)): layer l of a tile
+// accumulates into acc[l & 1], so layer l+1's MMAs start on chunk c of its
+// input as soon as the epilogue of layer l has written that chunk, while the
+// epilogue still drains acc[l & 1].  The activations are rewritten in place:
+// the epilogue of layer l starts only after every MMA of layer l (the
+// readers of the old activations) has completed.  acc_empty[a] tells the MMA
+// warp that all sixteen epilogue warps have finished their TMEM loads of
+// acc[a], before the next layer that accumulates there.
+//
+// Barrier phases (all parity waits, bounded): per tile acc_full[a] and
+// acc_empty[a] complete twice (layers a and a + 2), act_ready[c] three times
+// (inputs of layers 1-3), dot_bar[quadrant] once; none can run two phases
+// ahead of its waiter because each completion needs the waiter's previous
+// step (argued at each wait below).
+constexpr int SV_EPI_WARPS = 16;
+constexpr int SV_EPI = 32*SV_EPI_WARPS;                    // 512 epilogue threads
+constexpr int SV_MMA_WARP = SV_EPI_WARPS;
+constexpr int SV_PROD_WARP = SV_EPI_WARPS + 1;
+constexpr int SV_THREADS = SV_EPI + 64;
+constexpr int SV_COLS = KCI/(SV_EPI_WARPS/4);              // 8 columns of a chunk per warp
+constexpr int SV_PARAMS = 5*HID;                           // b[0..3], w_out (floats)
+constexpr int SV_SMEM = 2*ACT_BYTES + STAGES*CHUNK_BYTES + W0_BYTES + 4*X_BYTES + 4*SV_PARAMS;
+static_assert(SV_COLS == 8, "the epilogue moves one 16-byte unit per row and chunk");
+
+// z = acc + bias and h = silu(z) for 8 columns.
+__device__ __forceinline__ void sv_silu8(const uint32_t (&a)[8], const float *bias, float (&h)[8])
+{
+    const float4 b0 = *reinterpret_cast<const float4 *>(bias);
+    const float4 b1 = *reinterpret_cast<const float4 *>(bias + 4);
+    const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+    #pragma unroll
+    for (int j = 0; j < 8; ++j) h[j] = silu(__uint_as_float(a[j]) + bb[j]);
+}
+
+__global__ void __launch_bounds__(SV_THREADS, 1)
+mlp_serve(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
+          const __nv_bfloat16 *__restrict__ x_lo, InferParams prm, float *__restrict__ out,
+          int *__restrict__ err)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t *act = smem;
+    uint8_t *act_lo = smem + ACT_BYTES;
+    uint8_t *ring = smem + 2*ACT_BYTES;
+    uint8_t *w0 = ring + STAGES*CHUNK_BYTES;
+    uint8_t *xs = w0 + W0_BYTES;                  // [2 buffers][hi, lo] x X_BYTES
+    float *par = reinterpret_cast<float *>(xs + 4*X_BYTES);
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], act_ready[CHUNKS_PER_LAYER];
+    __shared__ __align__(8) uint64_t acc_full[2], acc_empty[2], dot_bar[4], w0_bar, drain;
+    __shared__ uint32_t tmem_slot;
+    __shared__ float dot_part[3][TM];
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int my_tiles = blockIdx.x < n_tiles ? (n_tiles - 1 - blockIdx.x)/gridDim.x + 1 : 0;
+
+    if (warp == 0) {
+        tc::tmem_alloc(&tmem_slot, 2*HID);
+        tc::tmem_relinquish();
+    }
+    if (t == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        for (int c = 0; c < CHUNKS_PER_LAYER; ++c) tc::mbar_init(&act_ready[c], SV_EPI_WARPS);
+        for (int a = 0; a < 2; ++a) {
+            tc::mbar_init(&acc_full[a], 1);
+            tc::mbar_init(&acc_empty[a], SV_EPI_WARPS);
+        }
+        for (int q = 0; q < 4; ++q) tc::mbar_init(&dot_bar[q], SV_EPI_WARPS/4 - 1);
+        tc::mbar_init(&w0_bar, 1);
+        tc::mbar_init(&drain, 1);
+        tc::mbar_fence_init();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == SV_PROD_WARP) {
+        // ---- producer: the weight chunks of every tile, in MMA order ----
+        if (lane == 0) {
+            bool ok = true;
+            tc::mbar_arrive_expect_tx(&w0_bar, W0_BYTES);
+            tc::bulk_load(w0, prm.img, W0_BYTES, &w0_bar);
+            const int total = my_tiles*CHUNKS_PER_TILE;
+            int i = 0;
+            for (; i < total; ++i) {
+                const int s = i % STAGES, use = i/STAGES;
+                if (use > 0 && !tc::mbar_wait(&empty[s], (uint32_t)((use - 1) & 1))) {
+                    ok = false;
+                    break;
+                }
+                tc::mbar_arrive_expect_tx(&full[s], CHUNK_BYTES);
+                tc::bulk_load(ring + s*CHUNK_BYTES,
+                              prm.img + W0_BYTES + (size_t)(i % CHUNKS_PER_TILE)*CHUNK_BYTES,
+                              CHUNK_BYTES, &full[s]);
+            }
+            for (int j = (i > STAGES ? i - STAGES : 0); j < i; ++j)
+                ok = tc::mbar_wait(&full[j % STAGES], (uint32_t)((j/STAGES) & 1)) && ok;
+            ok = tc::mbar_wait(&w0_bar, 0u) && ok;
+            if (!ok) atomicExch(err, 2);
+        }
+    } else if (warp == SV_MMA_WARP) {
+        // ---- MMA issue (lane 0) and feature loads (all lanes) ----
+        constexpr uint32_t idesc = tc::idesc_bf16(TM, HID);
+        const uint32_t a_hi = tc::smem_u32(act), a_lo = tc::smem_u32(act_lo);
+        auto load_x = [&](int k) {
+            uint8_t *xb = xs + (k & 1)*2*X_BYTES;
+            const int row0 = (blockIdx.x + k*gridDim.x)*TM;
+            for (int i = lane; i < 2*TM; i += 32) {
+                const int r = i >> 1, c = (i & 1)*8;
+                const size_t g = (size_t)(row0 + r)*NIN + c;
+                *reinterpret_cast<uint4 *>(xb + tc::kmajor_offset<TM>(r, c)) =
+                    *reinterpret_cast<const uint4 *>(x + g);
+                *reinterpret_cast<uint4 *>(xb + X_BYTES + tc::kmajor_offset<TM>(r, c)) =
+                    *reinterpret_cast<const uint4 *>(x_lo + g);
+            }
+            tc::fence_async_smem();
+            __syncwarp();
+        };
+        auto wait = [&](uint64_t *bar, uint32_t parity) {
+            return __all_sync(0xffffffffu, tc::mbar_wait(bar, parity)) != 0;
+        };
+        bool ok = true;
+        int chunk = 0;
+        if (my_tiles > 0) load_x(0);
+        ok = wait(&w0_bar, 0u);
+        for (int k = 0; k < my_tiles && ok; ++k) {
+            // layer 0 into acc[0]; its previous reader is the epilogue of
+            // layer 2 of tile k-1 (acc_empty[0] completion 2k-1, odd), which
+            // cannot complete again before this MMA is issued
+            if (k > 0 && !(ok = wait(&acc_empty[0], 1u))) break;
+            tc::fence_after_sync();
+            if (lane == 0) {
+                const uint32_t xb = tc::smem_u32(xs + (k & 1)*2*X_BYTES);
+                const uint64_t bdesc = tc::kmajor_desc<HID>(tc::smem_u32(w0), 0);
+                tc::mma_bf16(tmem, tc::kmajor_desc<TM>(xb, 0), bdesc, idesc, 0u);
+                tc::mma_bf16(tmem, tc::kmajor_desc<TM>(xb + X_BYTES, 0), bdesc, idesc, 1u);
+                tc::mma_commit(&acc_full[0]);
+            }
+            __syncwarp();
+            for (int l = 1; l < 4 && ok; ++l) {
+                const int a = l & 1;
+                const uint32_t d = tmem + (uint32_t)(HID*a);
+                // previous reader of acc[a]: layer 3 of tile k-1 for l = 1
+                // (completion 2k-1), layer l-2 of this tile for l = 2, 3
+                // (completion 2k)
+                if ((l >= 2 || k > 0) && !(ok = wait(&acc_empty[a], l >= 2 ? 0u : 1u))) break;
+                for (int c = 0; c < CHUNKS_PER_LAYER; ++c, ++chunk) {
+                    // chunk c of this layer's input: completion 3k + l - 1;
+                    // the next one needs this layer's acc_full, committed
+                    // below only after every chunk was consumed
+                    const int s = chunk % STAGES;
+                    if (!(ok = wait(&act_ready[c], (uint32_t)((3*k + l - 1) & 1))
+                               && wait(&full[s], (uint32_t)((chunk/STAGES) & 1))))
+                        break;
+                    tc::fence_after_sync();
+                    if (lane == 0) {
+                        const uint32_t b_addr = tc::smem_u32(ring + s*CHUNK_BYTES);
+                        #pragma unroll
+                        for (int st = 0; st < KCI/16; ++st) {
+                            const uint64_t bdesc = tc::kmajor_desc<HID>(b_addr, st);
+                            const int as = c*(KCI/16) + st;
+                            tc::mma_bf16(d, tc::kmajor_desc<TM>(a_hi, as), bdesc, idesc,
+                                         (c > 0 || st > 0) ? 1u : 0u);
+                            tc::mma_bf16(d, tc::kmajor_desc<TM>(a_lo, as), bdesc, idesc, 1u);
+                        }
+                        tc::mma_commit(&empty[s]);
+                    }
+                    __syncwarp();
+                }
+                if (!ok) break;
+                if (lane == 0) tc::mma_commit(&acc_full[a]);
+                __syncwarp();
+            }
+            // the features of the next tile go to the other buffer, last
+            // read by layer 0 of tile k-1, complete since layer 1's inputs
+            // of tile k-1 were produced from its result
+            if (ok && k + 1 < my_tiles) load_x(k + 1);
+        }
+        // every MMA issued has completed before TMEM is released
+        if (lane == 0) {
+            tc::mma_commit(&drain);
+            ok = tc::mbar_wait(&drain, 0u) && ok;
+            if (!ok) atomicExch(err, 3);
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue warps ----
+        for (int i = t; i < SV_PARAMS; i += SV_EPI)
+            par[i] = i < 4*HID ? prm.b[i/HID][i % HID] : prm.w_out[i - 4*HID];
+        tc::bar_sync(1, SV_EPI);
+        const float b_out = *prm.b_out;
+        const int quad = warp & 3, slot = warp >> 2;
+        const int row = 32*quad + lane;
+        const int cs = SV_COLS*slot;
+        const uint32_t lane_base = (uint32_t)(32*quad) << 16;
+        bool ok = true;
+        for (int k = 0; k < my_tiles && ok; ++k) {
+            const int row0 = (blockIdx.x + k*gridDim.x)*TM;
+            for (int l = 0; l < 4; ++l) {
+                const int a = l & 1;
+                // acc_full[a]: completion 2k + (l >> 1)
+                if (!(ok = __all_sync(0xffffffffu,
+                                      tc::mbar_wait(&acc_full[a], (uint32_t)(l >> 1))) != 0))
+                    break;
+                tc::fence_after_sync();
+                const uint32_t acc = tmem + lane_base + (uint32_t)(HID*a + cs);
+                const float *bias = par + l*HID + cs;
+                float dot = 0.0f;
+                uint32_t ra[8], rb[8];
+                tc::tmem_ld8(acc, ra);
+                tc::tmem_wait_ld8(ra);
+                #pragma unroll
+                for (int c = 0; c < CHUNKS_PER_LAYER; ++c) {
+                    if (c + 1 < CHUNKS_PER_LAYER) {
+                        tc::tmem_ld8(acc + (uint32_t)(KCI*(c + 1)), rb);
+                    } else {
+                        // all TMEM loads of acc[a] have completed
+                        tc::fence_before_sync();
+                        __syncwarp();
+                        if (lane == 0) tc::mbar_arrive(&acc_empty[a]);
+                    }
+                    float h[8];
+                    sv_silu8(ra, bias + KCI*c, h);
+                    if (l < 3) {
+                        uint4 hi, lo;
+                        uint32_t *hp = &hi.x, *lp = &lo.x;
+                        #pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const uint32_t u = pack2(h[2*j], h[2*j + 1]);
+                            hp[j] = u;
+                            lp[j] = pack2(h[2*j] - bf_lo(u), h[2*j + 1] - bf_hi(u));
+                        }
+                        const uint32_t off = tc::kmajor_offset<TM>(row, KCI*c + cs);
+                        *reinterpret_cast<uint4 *>(act + off) = hi;
+                        *reinterpret_cast<uint4 *>(act_lo + off) = lo;
+                        tc::fence_async_smem();
+                        __syncwarp();
+                        if (lane == 0) tc::mbar_arrive(&act_ready[c]);
+                    } else {
+                        const float *wo = par + 4*HID + KCI*c + cs;
+                        #pragma unroll
+                        for (int j = 0; j < 8; ++j) dot = fmaf(h[j], wo[j], dot);
+                    }
+                    if (c + 1 < CHUNKS_PER_LAYER) {
+                        tc::tmem_wait_ld8(rb);
+                        #pragma unroll
+                        for (int j = 0; j < 8; ++j) ra[j] = rb[j];
+                    }
+                }
+                if (l == 3) {
+                    // four partial sums per row; slot 0 adds them.  Slots
+                    // 1-3 write dot_part again only in the next tile's last
+                    // layer, which needs slot 0's activations of that tile.
+                    if (slot > 0) {
+                        dot_part[slot - 1][row] = dot;
+                        __syncwarp();
+                        if (lane == 0) tc::mbar_arrive(&dot_bar[quad]);
+                    } else {
+                        if (!(ok = __all_sync(0xffffffffu,
+                                              tc::mbar_wait(&dot_bar[quad], (uint32_t)(k & 1))) != 0))
+                            break;
+                        if (row0 + row < n)
+                            out[row0 + row] = ((dot + dot_part[0][row]) + dot_part[1][row])
+                                              + dot_part[2][row] + b_out;
+                    }
+                }
+            }
+        }
+        if (!ok && lane == 0) atomicExch(err, 1);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 2*HID);
+}
+
 // ---------------------------------------------------------------- backward --
 // mlp_backward_p: the backward pass through the three 256 x 256 layers as a
 // persistent, pipelined kernel with the structure of mlp_infer: a producer
@@ -1062,6 +1354,47 @@ int32_t sasb200_mlp_infer(int32_t n, int32_t n_pad, const void *x, const void *x
         n, n_tiles, static_cast<const __nv_bfloat16 *>(x),
         static_cast<const __nv_bfloat16 *>(x_lo), prm, out, err);
     return status("mlp_infer");
+}
+
+// Inference only: out[n] for x, x_lo [n_pad x 16] with the packed weights,
+// through the overlapped kernel (mlp_serve); persistent grid of at most
+// `blocks` CTAs (0 = one per SM).  err receives 1, 2 or 3 if a pipeline
+// wait ran out.
+int32_t sasb200_mlp_serve(int32_t n, int32_t n_pad, const void *x, const void *x_lo,
+                          const void *img, const float *const *b, const float *w_out,
+                          const float *b_out, float *out, int32_t *err, int32_t blocks,
+                          void *stream)
+{
+    errbuf()[0] = 0;
+    if (n < 0 || n_pad % TM || n > n_pad || !x || !x_lo || !img || !b || !w_out || !b_out
+        || !out || !err || blocks < 0)
+        return (std::snprintf(errbuf(), 256, "bad arguments"), -1);
+    if (reinterpret_cast<uintptr_t>(img) % 16)
+        return (std::snprintf(errbuf(), 256, "weight image must be 16-byte aligned"), -1);
+    for (int l = 0; l < 4; ++l)
+        if (!b[l] || reinterpret_cast<uintptr_t>(b[l]) % 4)
+            return (std::snprintf(errbuf(), 256, "bad bias pointer"), -1);
+    if (n_pad == 0) return 0;
+    InferParams prm;
+    prm.img = static_cast<const uint8_t *>(img);
+    for (int l = 0; l < 4; ++l) prm.b[l] = b[l];
+    prm.w_out = w_out;
+    prm.b_out = b_out;
+    prm.z_save = nullptr;
+    prm.h_save = nullptr;
+    const int n_tiles = n_pad/TM;
+    if (blocks == 0) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        blocks = sms > 0 ? sms : 1;
+    }
+    if (blocks > n_tiles) blocks = n_tiles;
+    cudaFuncSetAttribute(mlp_serve, cudaFuncAttributeMaxDynamicSharedMemorySize, SV_SMEM);
+    mlp_serve<<<blocks, SV_THREADS, SV_SMEM, (cudaStream_t)stream>>>(
+        n, n_tiles, static_cast<const __nv_bfloat16 *>(x),
+        static_cast<const __nv_bfloat16 *>(x_lo), prm, out, err);
+    return status("mlp_serve");
 }
 
 // out[n] (and z/h planes [4][n_pad x 256] when non-null) for x[n_pad x 16];

@@ -71,6 +71,12 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
                  :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
+// Arrive once (release at CTA scope).
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
+
 // ---- bulk copy (TMA engine, untiled, no multicast) --------------------------
 // global -> this CTA's shared memory, completion counted on *bar.  Both
 // addresses 16-byte aligned, bytes a multiple of 16.
@@ -148,6 +154,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
 __device__ __forceinline__ void tmem_wait_ld()
 {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// 32 TMEM lanes x 8 columns; tmem_wait_ld8 on the same registers completes
+// it (the registers are operands of the wait, so no use of them can be
+// scheduled before it).
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 "
+                 "{%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                   "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld8(uint32_t (&r)[8])
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                   "+r"(r[6]), "+r"(r[7])
+                 :: "memory");
 }
 
 // ---- MMA -------------------------------------------------------------------

@@ -59,12 +59,13 @@ def _lib():
     lib.sasb200_mlp_features.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P]
     lib.sasb200_mlp_pack.argtypes = [P, P, P, P, P, P]
     lib.sasb200_mlp_infer.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P, I, P]
+    lib.sasb200_mlp_serve.argtypes = [I, I, P, P, P, P, P, P, P, P, I, P]
     lib.sasb200_mlp_pack_t.argtypes = [P, P, P, P, P]
     lib.sasb200_mlp_backward_p.argtypes = [I, I, P, P, P, P, P, P, I, P]
     for name in ("sasb200_mlp_forward", "sasb200_mlp_backward", "sasb200_gemm_nt",
                  "sasb200_transpose_bf16", "sasb200_row_dot", "sasb200_loss_grad",
                  "sasb200_adam", "sasb200_mlp_features", "sasb200_mlp_pack",
-                 "sasb200_mlp_infer", "sasb200_mlp_image_bytes", "sasb200_mlp_pack_t",
+                 "sasb200_mlp_infer", "sasb200_mlp_serve", "sasb200_mlp_image_bytes", "sasb200_mlp_pack_t",
                  "sasb200_mlp_image_t_bytes", "sasb200_mlp_backward_p"):
         getattr(lib, name).restype = I
     lib.sasb200_mlp_last_error.restype = ct.c_char_p
@@ -181,6 +182,21 @@ class MLP:
             n, n_pad, x.data_ptr(), x_lo.data_ptr(), self.img.data_ptr(), self._ptrs(self.b),
             self.w_out.data_ptr(), self.b_out.data_ptr(), self._infer_out.data_ptr(), None, None,
             self.err.data_ptr(), int(blocks), self.stream.cuda_stream), "mlp_infer")
+        return self._infer_out[:n_pad]
+
+    def serve(self, x, x_lo, n, blocks=0):
+        """Inference only, through the overlapped kernel (mlp_serve): the
+        hidden activations of :meth:`infer` with the output dot summed in
+        another order; on self.stream."""
+        torch = self.torch
+        n_pad = x.shape[0]
+        if self._infer_out is None or self._infer_out.numel() < n_pad:
+            self._infer_out = torch.empty(n_pad, dtype=torch.float32, device=self.device)
+        self._pack()
+        self._check(self.lib.sasb200_mlp_serve(
+            n, n_pad, x.data_ptr(), x_lo.data_ptr(), self.img.data_ptr(), self._ptrs(self.b),
+            self.w_out.data_ptr(), self.b_out.data_ptr(), self._infer_out.data_ptr(),
+            self.err.data_ptr(), int(blocks), self.stream.cuda_stream), "mlp_serve")
         return self._infer_out[:n_pad]
 
     def forward(self, x, x_lo, n, save=False):

@@ -198,6 +198,41 @@ def test_tc_infer_matches_forward(cuda, n, blocks):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n, blocks", [(1, 0), (300, 0), (5000, 3), (128*300 + 17, 0),
+                                       (128*1000, 1)])
+def test_tc_serve_matches_infer(cuda, n, blocks):
+    """The overlapped inference kernel (its own MMA warp, two TMEM
+    accumulators, layer l+1's MMAs under layer l's epilogue) gives the
+    outputs of mlp_infer: the hidden activations are computed identically,
+    only the output dot is summed in four partial sums per row.  Cases: one
+    row, one tile per CTA, many tiles per CTA (every barrier phase wraps
+    many times), one CTA for 1000 tiles."""
+    import torch
+    from sasmodels_b200.surrogate import pad128
+    rng = np.random.default_rng(17)
+    net, W, b, w_out, b_out = _gpu_net(rng)
+    n_pad = pad128(n)
+    x, xlo, xh, _ = _inputs(rng, n, n_pad)
+    inf = net.infer(x, xlo, n)
+    net.stream.synchronize()
+    a = inf.cpu().numpy()[:n].copy()
+    net._infer_out.fill_(float("nan"))
+    torch.cuda.synchronize()
+    srv = net.serve(x, xlo, n, blocks=blocks)
+    net.stream.synchronize()
+    assert net.errors() == 0
+    c = srv.cpu().numpy()
+    assert np.isfinite(c[:n]).all()
+    np.testing.assert_allclose(c[:n], a, rtol=1e-5, atol=1e-6*np.abs(a).max())
+    # rows beyond n are not written
+    assert np.isnan(c[n:n_pad]).all()
+    ref, _, _ = mlp_ref.forward(xh[:min(n, 2000)], [mlp_ref.bf16(w) for w in W],
+                                [np.float32(v).astype(np.float64) for v in b],
+                                np.float32(w_out).astype(np.float64), np.float32(b_out))
+    assert np.abs(c[:len(ref)] - ref).max()/np.abs(ref).max() < 2e-3
+
+
+@pytest.mark.gpu
 def test_tc_infer_tracks_training(cuda):
     """The weight image is refreshed after training steps."""
     import torch
