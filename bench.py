@@ -911,11 +911,13 @@ def surrogate_extra(dev, n_train_sets=50000, epochs=32, gate_epochs=16, n_holdou
     the plain FP64 path on the same points."""
     from sasmodels_b200.surrogate import train_and_evaluate
     t0 = time.perf_counter()
-    _, rep = train_and_evaluate(n_train_sets=n_train_sets, nq=1000, epochs=epochs,
+    S, rep = train_and_evaluate(n_train_sets=n_train_sets, nq=1000, epochs=epochs,
                                 gate_epochs=gate_epochs, n_holdout_sets=n_holdout_sets,
                                 device=dev)
+    wall = time.perf_counter() - t0
     op = rep["operating_points"]["0.01"]
     return {"samples_per_s_at_1pct": op["samples_per_s"],
+            "mlp_kernels": mlp_kernel_times(S.net),
             "speedup_vs_plain_f64": op["speedup"],
             "speedup_vs_plain_f32c": op["speedup_vs_plain_f32c"],
             "fallback_frac": op["fallback_frac"], "frac_within_1pct": op["frac_within"],
@@ -923,9 +925,64 @@ def surrogate_extra(dev, n_train_sets=50000, epochs=32, gate_epochs=16, n_holdou
             "net_only_median_err": rep["net_median_err"], "net_only_p99_err": rep["net_p99_err"],
             "train_samples": rep["train_samples"], "epochs": rep["epochs"],
             "data_s": rep["data_s"], "train_s": rep["train_s"], "gate_s": rep["gate_s"],
-            "wall_s": time.perf_counter() - t0,
+            "wall_s": wall,
             "labels": "batched FP32c engine (within 1e-5 of FP64); judged by plain FP64",
             "report": rep}
+
+
+#: Multiply-adds of the surrogate network per row, counted as 2 flops each:
+#: 16 -> 256, three 256 -> 256 layers and the 256 -> 1 output (0.402 MFLOP).
+#: The kernels issue the hidden layers twice (the compensated hi and lo
+#: activations), which this algorithmic count leaves out.
+MLP_FLOPS_PER_ROW = 2*(16*256 + 3*256*256 + 256)
+
+
+def bf16_peak():
+    """Dense BF16 burst peak in TFLOP/s and where it comes from."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fid:
+            return float(json.load(fid)["bf16_tflops"]), "of measured (cuBLAS bf16 burst)"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "of fallback"
+
+
+def mlp_kernel_times(net, rows=4_000_000, reps=5):
+    """Device time of one inference launch over `rows` rows (features of
+    2 x 128 MB, more than L2) for the overlapped serving kernel (mlp_serve)
+    and the pipelined training forward without planes (mlp_infer), median of
+    `reps` CUDA-event timings on the network's stream after 3 warm-up
+    launches; algorithmic TFLOP/s from MLP_FLOPS_PER_ROW."""
+    import torch
+    from sasmodels_b200.surrogate import pad128
+    n_pad = pad128(rows)
+    g = torch.Generator(device=net.device).manual_seed(5)
+    x = (0.5*torch.randn(n_pad, 16, device=net.device, generator=g)).to(torch.bfloat16)
+    x_lo = (1e-3*torch.randn(n_pad, 16, device=net.device, generator=g)).to(torch.bfloat16)
+    peak, source = bf16_peak()
+    out = {"rows": rows, "mflop_per_row": MLP_FLOPS_PER_ROW/1e6, "peak_tflops": peak,
+           "peak_source": source}
+    torch.cuda.synchronize()
+    for name in ("serve", "infer"):
+        fn = getattr(net, name)
+        with torch.cuda.stream(net.stream):
+            for _ in range(3):
+                fn(x, x_lo, rows)
+            times = []
+            for _ in range(reps):
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+                ev[0].record(net.stream)
+                fn(x, x_lo, rows)
+                ev[1].record(net.stream)
+                ev[1].synchronize()
+                times.append(ev[0].elapsed_time(ev[1]))
+        ms = float(np.median(times))
+        got = rows*MLP_FLOPS_PER_ROW/(ms*1e-3)/1e12
+        out["mlp_" + name] = {"ms": ms, "rows_per_s": rows/(ms*1e-3),
+                              "algorithmic_tflops": got, "frac": got/peak}
+    if net.errors():
+        raise RuntimeError("surrogate kernel pipeline error %d" % net.errors())
+    return out
 
 
 def population_vs_dll(dev, stride=97, nq_sub=8, max_mesh=60000):
@@ -1113,6 +1170,7 @@ def run_surrogate(args, world, rank, local):
         "data": "synthetic (plain-kernel labels)",
         "config": {"workload": "polydisperse cylinder surrogate, 7 inputs -> 4x256 SiLU -> log I",
                    "train_samples": rep["train_samples"], "epochs": rep["epochs"]},
+        "mlp_kernels": mlp_kernel_times(S.net),
         "surrogate": rep,
     }
     print(json.dumps(line), flush=True)

@@ -49,7 +49,19 @@ struct Weights {
     const float *b_out;           // device scalar
 };
 
-__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+// silu(z) = z sigmoid(z) with sigmoid(z) = (1 + tanh(z/2))/2, i.e.
+// h = z/2 + (z/2) tanh(z/2): one MUFU operation (tanh.approx.f32, documented
+// maximum relative error about 2^-11) and two FP32 operations.  Every
+// forward kernel (training and serving) uses this one function, so the
+// network is served with the activation it was trained with.
+__device__ __forceinline__ float silu(float z)
+{
+    const float hz = 0.5f*z;
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(hz));
+    return fmaf(hz, t, hz);
+}
+
 __device__ __forceinline__ float dsilu(float z)
 {
     const float s = 1.0f/(1.0f + __expf(-z));
@@ -813,15 +825,22 @@ mlp_infer(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
 // hidden activations are bitwise those of mlp_infer; the output dot sums
 // the 256 columns in another order (four partial sums per row).
 //
-// Roles, 18 warps per CTA (one CTA per SM, persistent over 128-row tiles):
+// Roles, 19 warps per CTA (one CTA per SM, persistent over 128-row tiles):
 //   warps 0-15  epilogue.  Warp w reads the TMEM lanes of its quadrant
 //               (rows 32(w%4) .. +31) and, of every 32-column chunk, the 8
 //               columns at 8(w/4).  Chunk by chunk: bias + SiLU + split into
 //               the activation tile, then one arrive per warp on
 //               act_ready[chunk].
 //   warp 16     lane 0 issues every MMA; all lanes load the next tile's
-//               features while the tensor core runs the last layer.
+//               features while the tensor core runs the last layer.  An MMA
+//               issue holds its thread for about the tensor core's time for
+//               the previous MMA, so this lane does no barrier waits of its
+//               own for layers 1-3: it spins on a counter of ready chunks.
 //   warp 17     the bulk-copy producer of the weight ring (as mlp_infer).
+//   warp 18     the waiter: for every chunk of layers 1-3 in MMA order, waits
+//               for the accumulator to be free, the activations and the
+//               weights, then publishes the chunk (release store of the
+//               count of ready chunks).
 // Two TMEM accumulators (columns [0, 256) and [256, 512)): layer l of a tile
 // accumulates into acc[l & 1], so layer l+1's MMAs start on chunk c of its
 // input as soon as the epilogue of layer l has written that chunk, while the
@@ -840,11 +859,21 @@ constexpr int SV_EPI_WARPS = 16;
 constexpr int SV_EPI = 32*SV_EPI_WARPS;                    // 512 epilogue threads
 constexpr int SV_MMA_WARP = SV_EPI_WARPS;
 constexpr int SV_PROD_WARP = SV_EPI_WARPS + 1;
-constexpr int SV_THREADS = SV_EPI + 64;
+constexpr int SV_WAIT_WARP = SV_EPI_WARPS + 2;
+constexpr int SV_THREADS = SV_EPI + 96;
 constexpr int SV_COLS = KCI/(SV_EPI_WARPS/4);              // 8 columns of a chunk per warp
 constexpr int SV_PARAMS = 5*HID;                           // b[0..3], w_out (floats)
 constexpr int SV_SMEM = 2*ACT_BYTES + STAGES*CHUNK_BYTES + W0_BYTES + 4*X_BYTES + 4*SV_PARAMS;
+constexpr int SV_ROUND = 1;                                // chunks per epilogue round
 static_assert(SV_COLS == 8, "the epilogue moves one 16-byte unit per row and chunk");
+
+// Bounded wait by every lane of a warp on one mbarrier phase; the warp agrees
+// on the outcome.  (Polling by lane 0 alone with a shuffle of the outcome was
+// measured slower here.)
+__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity)
+{
+    return __all_sync(0xffffffffu, tc::mbar_wait(bar, parity)) != 0;
+}
 
 // z = acc + bias and h = silu(z) for 8 columns.
 __device__ __forceinline__ void sv_silu8(const uint32_t (&a)[8], const float *bias, float (&h)[8])
@@ -856,6 +885,7 @@ __device__ __forceinline__ void sv_silu8(const uint32_t (&a)[8], const float *bi
     for (int j = 0; j < 8; ++j) h[j] = silu(__uint_as_float(a[j]) + bb[j]);
 }
 
+template <int RND>
 __global__ void __launch_bounds__(SV_THREADS, 1)
 mlp_serve(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
           const __nv_bfloat16 *__restrict__ x_lo, InferParams prm, float *__restrict__ out,
@@ -870,7 +900,7 @@ mlp_serve(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
     float *par = reinterpret_cast<float *>(xs + 4*X_BYTES);
     __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], act_ready[CHUNKS_PER_LAYER];
     __shared__ __align__(8) uint64_t acc_full[2], acc_empty[2], dot_bar[4], w0_bar, drain;
-    __shared__ uint32_t tmem_slot;
+    __shared__ uint32_t tmem_slot, ready_seq;
     __shared__ float dot_part[3][TM];
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int my_tiles = blockIdx.x < n_tiles ? (n_tiles - 1 - blockIdx.x)/gridDim.x + 1 : 0;
@@ -892,6 +922,7 @@ mlp_serve(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
         for (int q = 0; q < 4; ++q) tc::mbar_init(&dot_bar[q], SV_EPI_WARPS/4 - 1);
         tc::mbar_init(&w0_bar, 1);
         tc::mbar_init(&drain, 1);
+        ready_seq = 0;
         tc::mbar_fence_init();
     }
     tc::fence_before_sync();
@@ -923,6 +954,33 @@ mlp_serve(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
             ok = tc::mbar_wait(&w0_bar, 0u) && ok;
             if (!ok) atomicExch(err, 2);
         }
+    } else if (warp == SV_WAIT_WARP) {
+        // ---- waiter: readiness of every chunk of layers 1-3, in MMA order ----
+        // A chunk is ready when its accumulator is free (chunk 0 of a layer),
+        // its input activations are written and its weights have landed;
+        // the count of ready chunks is published with a release store that
+        // the MMA lane reads with acquire loads.
+        bool ok = true;
+        int chunk = 0;
+        for (int k = 0; k < my_tiles && ok; ++k) {
+            for (int l = 1; l < 4 && ok; ++l) {
+                const int a = l & 1;
+                // previous reader of acc[a]: layer 3 of tile k-1 for l = 1
+                // (completion 2k-1), layer l-2 of this tile for l = 2, 3
+                // (completion 2k); the next completion needs this layer's
+                // MMAs, which wait for what is published here
+                if ((l >= 2 || k > 0) && !(ok = warp_wait(&acc_empty[a], l >= 2 ? 0u : 1u)))
+                    break;
+                for (int c = 0; c < CHUNKS_PER_LAYER; ++c, ++chunk) {
+                    // chunk c of this layer's input: completion 3k + l - 1
+                    if (!(ok = warp_wait(&act_ready[c], (uint32_t)((3*k + l - 1) & 1))
+                               && warp_wait(&full[chunk % STAGES], (uint32_t)((chunk/STAGES) & 1))))
+                        break;
+                    if (lane == 0) tc::st_release_shared(&ready_seq, (uint32_t)(chunk + 1));
+                }
+            }
+        }
+        if (!ok && lane == 0) atomicExch(err, 4);
     } else if (warp == SV_MMA_WARP) {
         // ---- MMA issue (lane 0) and feature loads (all lanes) ----
         constexpr uint32_t idesc = tc::idesc_bf16(TM, HID);
@@ -941,18 +999,15 @@ mlp_serve(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
             tc::fence_async_smem();
             __syncwarp();
         };
-        auto wait = [&](uint64_t *bar, uint32_t parity) {
-            return __all_sync(0xffffffffu, tc::mbar_wait(bar, parity)) != 0;
-        };
         bool ok = true;
         int chunk = 0;
         if (my_tiles > 0) load_x(0);
-        ok = wait(&w0_bar, 0u);
+        ok = warp_wait(&w0_bar, 0u);
         for (int k = 0; k < my_tiles && ok; ++k) {
             // layer 0 into acc[0]; its previous reader is the epilogue of
             // layer 2 of tile k-1 (acc_empty[0] completion 2k-1, odd), which
             // cannot complete again before this MMA is issued
-            if (k > 0 && !(ok = wait(&acc_empty[0], 1u))) break;
+            if (k > 0 && !(ok = warp_wait(&acc_empty[0], 1u))) break;
             tc::fence_after_sync();
             if (lane == 0) {
                 const uint32_t xb = tc::smem_u32(xs + (k & 1)*2*X_BYTES);
@@ -960,25 +1015,16 @@ mlp_serve(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
                 tc::mma_bf16(tmem, tc::kmajor_desc<TM>(xb, 0), bdesc, idesc, 0u);
                 tc::mma_bf16(tmem, tc::kmajor_desc<TM>(xb + X_BYTES, 0), bdesc, idesc, 1u);
                 tc::mma_commit(&acc_full[0]);
-            }
-            __syncwarp();
-            for (int l = 1; l < 4 && ok; ++l) {
-                const int a = l & 1;
-                const uint32_t d = tmem + (uint32_t)(HID*a);
-                // previous reader of acc[a]: layer 3 of tile k-1 for l = 1
-                // (completion 2k-1), layer l-2 of this tile for l = 2, 3
-                // (completion 2k)
-                if ((l >= 2 || k > 0) && !(ok = wait(&acc_empty[a], l >= 2 ? 0u : 1u))) break;
-                for (int c = 0; c < CHUNKS_PER_LAYER; ++c, ++chunk) {
-                    // chunk c of this layer's input: completion 3k + l - 1;
-                    // the next one needs this layer's acc_full, committed
-                    // below only after every chunk was consumed
-                    const int s = chunk % STAGES;
-                    if (!(ok = wait(&act_ready[c], (uint32_t)((3*k + l - 1) & 1))
-                               && wait(&full[s], (uint32_t)((chunk/STAGES) & 1))))
-                        break;
-                    tc::fence_after_sync();
-                    if (lane == 0) {
+                // layers 1-3: each chunk as soon as the waiter has published
+                // it.  An MMA issue holds this thread about as long as the
+                // tensor core takes for the previous one, so nothing else
+                // runs on this thread between chunks.
+                for (int l = 1; l < 4 && ok; ++l) {
+                    const uint32_t d = tmem + (uint32_t)(HID*(l & 1));
+                    for (int c = 0; c < CHUNKS_PER_LAYER; ++c, ++chunk) {
+                        if (!(ok = tc::spin_acquire_ge(&ready_seq, (uint32_t)(chunk + 1)))) break;
+                        tc::fence_after_sync();
+                        const int s = chunk % STAGES;
                         const uint32_t b_addr = tc::smem_u32(ring + s*CHUNK_BYTES);
                         #pragma unroll
                         for (int st = 0; st < KCI/16; ++st) {
@@ -990,12 +1036,11 @@ mlp_serve(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
                         }
                         tc::mma_commit(&empty[s]);
                     }
-                    __syncwarp();
+                    if (ok) tc::mma_commit(&acc_full[l & 1]);
                 }
-                if (!ok) break;
-                if (lane == 0) tc::mma_commit(&acc_full[a]);
-                __syncwarp();
             }
+            ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+            chunk = __shfl_sync(0xffffffffu, chunk, 0);
             // the features of the next tile go to the other buffer, last
             // read by layer 0 of tile k-1, complete since layer 1's inputs
             // of tile k-1 were produced from its result
@@ -1024,52 +1069,75 @@ mlp_serve(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
             for (int l = 0; l < 4; ++l) {
                 const int a = l & 1;
                 // acc_full[a]: completion 2k + (l >> 1)
-                if (!(ok = __all_sync(0xffffffffu,
-                                      tc::mbar_wait(&acc_full[a], (uint32_t)(l >> 1))) != 0))
+                if (!(ok = warp_wait(&acc_full[a], (uint32_t)(l >> 1))))
                     break;
                 tc::fence_after_sync();
                 const uint32_t acc = tmem + lane_base + (uint32_t)(HID*a + cs);
                 const float *bias = par + l*HID + cs;
                 float dot = 0.0f;
-                uint32_t ra[8], rb[8];
-                tc::tmem_ld8(acc, ra);
-                tc::tmem_wait_ld8(ra);
+                // RND chunks per round: their TMEM loads are issued together,
+                // one round ahead of the arithmetic, and one proxy fence
+                // covers their stores
+                uint32_t ra[RND][8], rb[RND][8];
                 #pragma unroll
-                for (int c = 0; c < CHUNKS_PER_LAYER; ++c) {
-                    if (c + 1 < CHUNKS_PER_LAYER) {
-                        tc::tmem_ld8(acc + (uint32_t)(KCI*(c + 1)), rb);
+                for (int r = 0; r < RND; ++r) tc::tmem_ld8(acc + (uint32_t)(KCI*r), ra[r]);
+                #pragma unroll
+                for (int r = 0; r < RND; ++r) tc::tmem_wait_ld8(ra[r]);
+                #pragma unroll
+                for (int j = 0; j < CHUNKS_PER_LAYER/RND; ++j) {
+                    const bool more = j + 1 < CHUNKS_PER_LAYER/RND;
+                    if (more) {
+                        #pragma unroll
+                        for (int r = 0; r < RND; ++r)
+                            tc::tmem_ld8(acc + (uint32_t)(KCI*(RND*(j + 1) + r)), rb[r]);
                     } else {
                         // all TMEM loads of acc[a] have completed
                         tc::fence_before_sync();
                         __syncwarp();
                         if (lane == 0) tc::mbar_arrive(&acc_empty[a]);
                     }
-                    float h[8];
-                    sv_silu8(ra, bias + KCI*c, h);
-                    if (l < 3) {
-                        uint4 hi, lo;
-                        uint32_t *hp = &hi.x, *lp = &lo.x;
-                        #pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            const uint32_t u = pack2(h[2*j], h[2*j + 1]);
-                            hp[j] = u;
-                            lp[j] = pack2(h[2*j] - bf_lo(u), h[2*j + 1] - bf_hi(u));
+                    #pragma unroll
+                    for (int r = 0; r < RND; ++r) {
+                        const int c = RND*j + r;
+                        float h[8];
+                        sv_silu8(ra[r], bias + KCI*c, h);
+                        if (l < 3) {
+                            uint4 hi, lo;
+                            uint32_t *hp = &hi.x, *lp = &lo.x;
+                            #pragma unroll
+                            for (int e = 0; e < 4; ++e) {
+                                const uint32_t u = pack2(h[2*e], h[2*e + 1]);
+                                hp[e] = u;
+                                lp[e] = pack2(h[2*e] - bf_lo(u), h[2*e + 1] - bf_hi(u));
+                            }
+                            const uint32_t off = tc::kmajor_offset<TM>(row, KCI*c + cs);
+                            *reinterpret_cast<uint4 *>(act + off) = hi;
+                            *reinterpret_cast<uint4 *>(act_lo + off) = lo;
+                        } else {
+                            const float *wp = par + 4*HID + KCI*c + cs;
+                            const float4 w0v = *reinterpret_cast<const float4 *>(wp);
+                            const float4 w1v = *reinterpret_cast<const float4 *>(wp + 4);
+                            const float wo[8] = {w0v.x, w0v.y, w0v.z, w0v.w,
+                                                 w1v.x, w1v.y, w1v.z, w1v.w};
+                            #pragma unroll
+                            for (int e = 0; e < 8; ++e) dot = fmaf(h[e], wo[e], dot);
                         }
-                        const uint32_t off = tc::kmajor_offset<TM>(row, KCI*c + cs);
-                        *reinterpret_cast<uint4 *>(act + off) = hi;
-                        *reinterpret_cast<uint4 *>(act_lo + off) = lo;
+                    }
+                    if (l < 3) {
                         tc::fence_async_smem();
                         __syncwarp();
-                        if (lane == 0) tc::mbar_arrive(&act_ready[c]);
-                    } else {
-                        const float *wo = par + 4*HID + KCI*c + cs;
-                        #pragma unroll
-                        for (int j = 0; j < 8; ++j) dot = fmaf(h[j], wo[j], dot);
+                        if (lane == 0) {
+                            #pragma unroll
+                            for (int r = 0; r < RND; ++r) tc::mbar_arrive(&act_ready[RND*j + r]);
+                        }
                     }
-                    if (c + 1 < CHUNKS_PER_LAYER) {
-                        tc::tmem_wait_ld8(rb);
+                    if (more) {
                         #pragma unroll
-                        for (int j = 0; j < 8; ++j) ra[j] = rb[j];
+                        for (int r = 0; r < RND; ++r) {
+                            tc::tmem_wait_ld8(rb[r]);
+                            #pragma unroll
+                            for (int e = 0; e < 8; ++e) ra[r][e] = rb[r][e];
+                        }
                     }
                 }
                 if (l == 3) {
@@ -1081,8 +1149,7 @@ mlp_serve(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
                         __syncwarp();
                         if (lane == 0) tc::mbar_arrive(&dot_bar[quad]);
                     } else {
-                        if (!(ok = __all_sync(0xffffffffu,
-                                              tc::mbar_wait(&dot_bar[quad], (uint32_t)(k & 1))) != 0))
+                        if (!(ok = warp_wait(&dot_bar[quad], (uint32_t)(k & 1))))
                             break;
                         if (row0 + row < n)
                             out[row0 + row] = ((dot + dot_part[0][row]) + dot_part[1][row])
@@ -1390,8 +1457,8 @@ int32_t sasb200_mlp_serve(int32_t n, int32_t n_pad, const void *x, const void *x
         blocks = sms > 0 ? sms : 1;
     }
     if (blocks > n_tiles) blocks = n_tiles;
-    cudaFuncSetAttribute(mlp_serve, cudaFuncAttributeMaxDynamicSharedMemorySize, SV_SMEM);
-    mlp_serve<<<blocks, SV_THREADS, SV_SMEM, (cudaStream_t)stream>>>(
+    cudaFuncSetAttribute(mlp_serve<SV_ROUND>, cudaFuncAttributeMaxDynamicSharedMemorySize, SV_SMEM);
+    mlp_serve<SV_ROUND><<<blocks, SV_THREADS, SV_SMEM, (cudaStream_t)stream>>>(
         n, n_tiles, static_cast<const __nv_bfloat16 *>(x),
         static_cast<const __nv_bfloat16 *>(x_lo), prm, out, err);
     return status("mlp_serve");

@@ -77,6 +77,25 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
 }
 
+// ---- release/acquire flags in shared memory ------------------------------
+__device__ __forceinline__ uint32_t ld_acquire_shared(const uint32_t *p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_shared(uint32_t *p, uint32_t v)
+{
+    asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" :: "r"(smem_u32(p)), "r"(v) : "memory");
+}
+// Bounded spin until *p >= target (acquire).
+__device__ __forceinline__ bool spin_acquire_ge(const uint32_t *p, uint32_t target)
+{
+    for (uint32_t i = 0; i < WAIT_LIMIT; ++i)
+        if (ld_acquire_shared(p) >= target) return true;
+    return false;
+}
+
 // ---- bulk copy (TMA engine, untiled, no multicast) --------------------------
 // global -> this CTA's shared memory, completion counted on *bar.  Both
 // addresses 16-byte aligned, bytes a multiple of 16.

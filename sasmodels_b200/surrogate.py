@@ -65,8 +65,8 @@ def _lib():
     for name in ("sasb200_mlp_forward", "sasb200_mlp_backward", "sasb200_gemm_nt",
                  "sasb200_transpose_bf16", "sasb200_row_dot", "sasb200_loss_grad",
                  "sasb200_adam", "sasb200_mlp_features", "sasb200_mlp_pack",
-                 "sasb200_mlp_infer", "sasb200_mlp_serve", "sasb200_mlp_image_bytes", "sasb200_mlp_pack_t",
-                 "sasb200_mlp_image_t_bytes", "sasb200_mlp_backward_p"):
+                 "sasb200_mlp_infer", "sasb200_mlp_serve", "sasb200_mlp_image_bytes",
+                 "sasb200_mlp_pack_t", "sasb200_mlp_image_t_bytes", "sasb200_mlp_backward_p"):
         getattr(lib, name).restype = I
     lib.sasb200_mlp_last_error.restype = ct.c_char_p
     return lib
@@ -617,10 +617,10 @@ class Surrogate:
         torch = self.torch
         x, x_lo, n = self._x(cols)
         with torch.cuda.stream(self.net.stream):
-            out = self.net.infer(x, x_lo, n)[:n].double()*self.y_std + self.y_mean
+            out = self.net.serve(x, x_lo, n)[:n].double()*self.y_std + self.y_mean
             g = None
             if gate and self.gate is not None:
-                g = self.gate.infer(x, x_lo, n)[:n].double()*self.g_std + self.g_mean
+                g = self.gate.serve(x, x_lo, n)[:n].double()*self.g_std + self.g_mean
             out = out.cpu()
             g = g.cpu() if g is not None else None
         self.net.stream.synchronize()
@@ -710,11 +710,11 @@ class Surrogate:
             q = torch.as_tensor(np.ascontiguousarray(cols["q"], 'd'), device=dev)
             x, x_lo, _ = self.net.features(T[:, 0], T[:, 1], T[:, 2], T[:, 3], T[:, 4], q,
                                            T[:, 5])
-            logi = (self.net.infer(x, x_lo, n)[:n].double()*self.y_std + self.y_mean
+            logi = (self.net.serve(x, x_lo, n)[:n].double()*self.y_std + self.y_mean
                     + 2.0*torch.log(T[:, 4].abs()))
             accept = (T[:, 6] > 0.5) & (q >= qlo) & (q <= qhi)
             if np.isfinite(thr):
-                g = self.gate.infer(x, x_lo, n)[:n].double()*self.g_std + self.g_mean
+                g = self.gate.serve(x, x_lo, n)[:n].double()*self.g_std + self.g_mean
                 accept &= g <= thr
             else:
                 accept &= False
