@@ -23,6 +23,7 @@ same workload per step; rank 0 only.
 """
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -500,6 +501,9 @@ def run_b200(args, world, rank, local):
             return I
 
         e2e_step()
+        # the setup's garbage is collected before the clock starts; the
+        # collector stays on while the steps are timed
+        gc.collect()
         barrier()
         with ClockSampler(local, "_e2e") as e2e_clocks:
             t0 = time.perf_counter()

@@ -71,11 +71,31 @@ def locality_order(qx, qy, bits=10):
     return np.argsort(code, kind="stable")
 
 
+def locality_order_device(qx, qy, bits=10):
+    """:func:`locality_order` computed where the tensors live (same
+    quantisation, round-half-even, bit interleave and stable sort, so the
+    same permutation); returns an int64 tensor on their device."""
+    torch = _torch()
+
+    def quantise(v):
+        lo, hi = v.min(), v.max()
+        span = hi - lo
+        scale = torch.where(span > 0, (2**bits - 1)/span, torch.zeros_like(span))
+        return torch.round((v - lo)*scale).to(torch.int64)
+    ix, iy = quantise(qx), quantise(qy)
+    code = torch.zeros_like(ix)
+    for b in range(bits):
+        code |= ((ix >> b) & 1) << (2*b)
+        code |= ((iy >> b) & 1) << (2*b + 1)
+    return torch.argsort(code, stable=True)
+
+
 class QInput:
     """q points for one kernel: 1D ``q`` or interleaved ``(qx, qy)`` pairs,
     uploaded once (``kernelcuda.py:386-422`` does the same per make_kernel).
-    2D points are uploaded in :func:`locality_order` (``order[i]`` is the
-    caller's index of device slot i); results are put back in caller order."""
+    2D points are uploaded in caller order and permuted on the device into
+    :func:`locality_order` (``order_dev[i]`` is the caller's index of device
+    slot i); results are put back in caller order on the device."""
 
     def __init__(self, q_vectors, device, reorder=True):
         torch = _torch()
@@ -83,12 +103,10 @@ class QInput:
         self.q_vectors = q_vectors
         self.nq = int(q_vectors[0].size)
         self.is_2d = len(q_vectors) == 2
-        self.order = None
+        self.order_dev = None
+        self._order = None
         if self.is_2d:
             qx, qy = q_vectors
-            if reorder and self.nq > 32:
-                self.order = locality_order(qx, qy)
-                qx, qy = qx[self.order], qy[self.order]
             q = np.empty(2*self.nq, 'd')
             q[0::2] = qx
             q[1::2] = qy
@@ -96,12 +114,24 @@ class QInput:
             q = q_vectors[0]
         else:
             raise ValueError("q_vectors must be [q] or [qx, qy]")
-        self.q = q
-        self.order_dev = (torch.as_tensor(self.order, device=device)
-                          if self.order is not None else None)
         self.dtype = np.dtype('d')
-        self.q_dev = torch.as_tensor(q, device=device) if self.nq else \
-            torch.zeros(2, dtype=torch.float64, device=device)
+        if not self.nq:
+            self.q_dev = torch.zeros(2, dtype=torch.float64, device=device)
+            return
+        q_dev = torch.as_tensor(q, device=device)
+        if self.is_2d and reorder and self.nq > 32:
+            pairs = q_dev.view(self.nq, 2)
+            self.order_dev = locality_order_device(pairs[:, 0], pairs[:, 1])
+            q_dev = pairs.index_select(0, self.order_dev).reshape(-1)
+        self.q_dev = q_dev
+
+    @property
+    def order(self):
+        """Host copy of ``order_dev`` (None when the points keep their
+        order)."""
+        if self._order is None and self.order_dev is not None:
+            self._order = self.order_dev.cpu().numpy()
+        return self._order
 
     def release(self):
         self.q_dev = None
@@ -187,6 +217,7 @@ class B200Kernel(_KernelBase):
             self._result_pin = torch.empty(nq*nout + 4, dtype=torch.float64,
                                            pin_memory=True)
         self._ws = None
+        self._result_caller = None
         self._pin_values = None
         self._pin_details = None
         self._dev_values = None
@@ -270,14 +301,19 @@ class B200Kernel(_KernelBase):
         with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
             self.launch(self.variant(magnetic), dev_d, dev_v, 0,
                         call_details.num_eval, cutoff, radius_effective_mode)
-            n = self._result_dev.numel()
-            self._result_pin[:n].copy_(self._result_dev, non_blocking=True)
+            res = self._result_dev
+            order = self.q_input.order_dev
+            if order is not None:
+                # slot i holds the caller's point order[i]
+                nq = self.q_input.nq
+                if self._result_caller is None:
+                    self._result_caller = torch.empty_like(res)
+                self._result_caller[nq:] = res[nq:]
+                self._result_caller[:nq].index_copy_(0, order, res[:nq])
+                res = self._result_caller
+            self._result_pin[:res.numel()].copy_(res, non_blocking=True)
         self.stream.synchronize()
         self.result[:] = self._result_pin.numpy()
-        order = self.q_input.order
-        if order is not None:
-            nq = self.q_input.nq
-            self.result[order] = self._result_pin.numpy()[:nq]
 
     # ------------------------------------------- reference engine interface --
     def Iq(self, call_details, values, cutoff, magnetic):
@@ -337,6 +373,7 @@ class B200Kernel(_KernelBase):
 
     def release(self):
         self._ws = None
+        self._result_caller = None
         if self.q_input is not None:
             self.q_input.release()
 

@@ -322,3 +322,18 @@ def test_support_libraries_export_header_symbols(lib_name):
     lib = ct.CDLL(os.path.join(_abi.LIB_DIR, "libsasb200_%s.so" % lib_name))
     for n in want:
         getattr(lib, n)
+
+
+def test_device_locality_order_matches_host():
+    """The Morton order computed with tensor operations (run here on the
+    CPU; on the GPU in make_kernel) is the host function's permutation,
+    ties included, and is a permutation."""
+    import torch
+    from sasmodels_b200.kernel import locality_order, locality_order_device
+    rng = np.random.default_rng(9)
+    for qx, qy in ((rng.uniform(-0.3, 0.5, 5000), rng.uniform(-0.1, 0.1, 5000)),
+                   (np.repeat(np.linspace(-1, 1, 64), 64), np.tile(np.linspace(-1, 1, 64), 64)),
+                   (np.full(100, 0.25), rng.uniform(0, 1, 100))):
+        want = locality_order(qx, qy)
+        got = locality_order_device(torch.as_tensor(qx), torch.as_tensor(qy)).numpy()
+        np.testing.assert_array_equal(got, want)
