@@ -91,6 +91,17 @@ int32_t sasb200_adam(int32_t size, int32_t splits, const float *grad, float *p, 
                      float *v, float lr, float b1, float b2, float eps, int32_t step, void *w,
                      void *wt, int32_t rows, int32_t cols, void *stream);
 
+/* the same Adam update with lr and the bias corrections read from the device
+ * (sched = {lr, 1 - b1^t, 1 - b2^t}), and the kernel that writes them:
+ * counters = {schedule step s, Adam step count t} (int32, device), lr = lr0
+ * min(1, (s + 1)/warmup) (1 + cos(pi s/total))/2, then s and t advance by
+ * one.  A CUDA graph of a whole training step replays with these. */
+int32_t sasb200_adam_sched(int32_t size, int32_t splits, const float *grad, float *p, float *m,
+                           float *v, const float *sched, float b1, float b2, float eps,
+                           void *w, void *wt, int32_t rows, int32_t cols, void *stream);
+int32_t sasb200_lr_schedule(int32_t *counters, float *sched, int32_t total, int32_t warmup,
+                            float lr0, float b1, float b2, void *stream);
+
 /* libsasb200_peaks.so: dependent-chain throughput probes (FP64 FMA, FP32
  * FMA, MUFU sine) whose measured rates are the roofline peaks of the
  * FP64 and FP32-compensated kernels. */

@@ -480,13 +480,22 @@ __global__ void loss_grad(int n, int n_pad, const float *__restrict__ out,
 
 // Adam on one FP32 master tensor; grad = sum of `splits` partial gradients.
 // Writes the BF16 copy (and its transpose if wt != nullptr, rows x cols).
+// sched (optional, device): {lr, bc1, bc2} of this step, written by
+// lr_schedule; replaces the by-value lr, bc1, bc2 (a CUDA graph of a
+// training step then replays with the schedule advancing on the device).
 __global__ void adam_step(int size, int splits, const float *__restrict__ grad, float *__restrict__ p,
                           float *__restrict__ m, float *__restrict__ v, float lr, float b1,
                           float b2, float eps, float bc1, float bc2, __nv_bfloat16 *__restrict__ w,
-                          __nv_bfloat16 *__restrict__ wt, int rows, int cols)
+                          __nv_bfloat16 *__restrict__ wt, int rows, int cols,
+                          const float *__restrict__ sched)
 {
     const int i = blockIdx.x*blockDim.x + threadIdx.x;
     if (i >= size) return;
+    if (sched) {
+        lr = sched[0];
+        bc1 = sched[1];
+        bc2 = sched[2];
+    }
     float g = 0.0f;
     for (int s = 0; s < splits; ++s) g += grad[(size_t)s*size + i];
     const float mi = b1*m[i] + (1.0f - b1)*g;
@@ -500,6 +509,25 @@ __global__ void adam_step(int size, int splits, const float *__restrict__ grad, 
         const int r = i/cols, c = i % cols;
         wt[(size_t)c*rows + r] = __float2bfloat16_rn(pi);
     }
+}
+
+// One training step's learning rate and Adam bias corrections from two
+// device counters {schedule step s, Adam step count t}, then s and t advance:
+// lr = lr0 min(1, (s + 1)/warmup) (1 + cos(pi s/total))/2 (linear warm-up,
+// cosine decay), bc1 = 1 - b1^(t+1), bc2 = 1 - b2^(t+1).  One thread.
+__global__ void lr_schedule(int *__restrict__ counters, float *__restrict__ sched, int total,
+                            int warmup, float lr0, float b1, float b2)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int s = counters[0], t = counters[1] + 1;
+    const double frac = (double)s/(double)total;
+    const double rate = (double)lr0*fmin(1.0, (double)(s + 1)/(double)warmup)
+                      *0.5*(1.0 + cos(3.141592653589793*frac));
+    sched[0] = (float)rate;
+    sched[1] = 1.0f - powf(b1, (float)t);
+    sched[2] = 1.0f - powf(b2, (float)t);
+    counters[0] = s + 1;
+    counters[1] = t;
 }
 
 // Surrogate input features, each mapped to about [-1, 1]: the seven model
@@ -1577,8 +1605,30 @@ int32_t sasb200_adam(int32_t size, int32_t splits, const float *grad, float *p, 
     const float bc1 = 1.0f - powf(b1, (float)step), bc2 = 1.0f - powf(b2, (float)step);
     adam_step<<<(size + 255)/256, 256, 0, (cudaStream_t)stream>>>(
         size, splits, grad, p, m, v, lr, b1, b2, eps, bc1, bc2,
-        static_cast<__nv_bfloat16 *>(w), static_cast<__nv_bfloat16 *>(wt), rows, cols);
+        static_cast<__nv_bfloat16 *>(w), static_cast<__nv_bfloat16 *>(wt), rows, cols, nullptr);
     return status("adam_step");
+}
+
+// Adam with lr and bias corrections read from the device (sched = {lr, bc1,
+// bc2}, written by sasb200_lr_schedule on the same stream).
+int32_t sasb200_adam_sched(int32_t size, int32_t splits, const float *grad, float *p, float *m,
+                           float *v, const float *sched, float b1, float b2, float eps, void *w,
+                           void *wt, int32_t rows, int32_t cols, void *stream)
+{
+    if (size <= 0 || splits <= 0 || !grad || !p || !m || !v || !sched) return -1;
+    if (wt && rows*cols != size) return -1;
+    adam_step<<<(size + 255)/256, 256, 0, (cudaStream_t)stream>>>(
+        size, splits, grad, p, m, v, 0.0f, b1, b2, eps, 1.0f, 1.0f,
+        static_cast<__nv_bfloat16 *>(w), static_cast<__nv_bfloat16 *>(wt), rows, cols, sched);
+    return status("adam_step");
+}
+
+int32_t sasb200_lr_schedule(int32_t *counters, float *sched, int32_t total, int32_t warmup,
+                            float lr0, float b1, float b2, void *stream)
+{
+    if (!counters || !sched || total <= 0 || warmup <= 0) return -1;
+    lr_schedule<<<1, 32, 0, (cudaStream_t)stream>>>(counters, sched, total, warmup, lr0, b1, b2);
+    return status("lr_schedule");
 }
 
 int32_t sasb200_mlp_features(int32_t n, int32_t n_pad, const double *radius, const double *length,

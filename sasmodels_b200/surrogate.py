@@ -41,6 +41,8 @@ TM = 128
 DOMAIN = dict(radius=(10.0, 300.0), length=(20.0, 3000.0), rpd=(0.0, 0.3),
               lpd=(0.0, 0.3), contrast=(-5.0, 5.0), q=(1e-3, 0.5))
 PD_N = 35
+#: linear learning-rate warm-up of the training schedule, in steps
+WARMUP_STEPS = 200
 
 
 def _lib():
@@ -56,6 +58,8 @@ def _lib():
     lib.sasb200_row_dot.argtypes = [I, I, P, P, P, P]
     lib.sasb200_loss_grad.argtypes = [I, I, P, P, F, P, P, P]
     lib.sasb200_adam.argtypes = [I, I, P, P, P, P, F, F, F, F, I, P, P, I, I, P]
+    lib.sasb200_adam_sched.argtypes = [I, I, P, P, P, P, P, F, F, F, P, P, I, I, P]
+    lib.sasb200_lr_schedule.argtypes = [P, P, I, I, F, F, F, P]
     lib.sasb200_mlp_features.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P]
     lib.sasb200_mlp_pack.argtypes = [P, P, P, P, P, P]
     lib.sasb200_mlp_infer.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P, I, P]
@@ -66,7 +70,8 @@ def _lib():
                  "sasb200_transpose_bf16", "sasb200_row_dot", "sasb200_loss_grad",
                  "sasb200_adam", "sasb200_mlp_features", "sasb200_mlp_pack",
                  "sasb200_mlp_infer", "sasb200_mlp_serve", "sasb200_mlp_image_bytes",
-                 "sasb200_mlp_pack_t", "sasb200_mlp_image_t_bytes", "sasb200_mlp_backward_p"):
+                 "sasb200_mlp_pack_t", "sasb200_mlp_image_t_bytes", "sasb200_mlp_backward_p",
+                 "sasb200_adam_sched", "sasb200_lr_schedule"):
         getattr(lib, name).restype = I
     lib.sasb200_mlp_last_error.restype = ct.c_char_p
     return lib
@@ -162,13 +167,16 @@ class MLP:
         key = (self.step_count, self._wversion)
         if self._packed == key:
             return
+        self._pack_kernels()
+        self._packed = key
+
+    def _pack_kernels(self):
         self._check(self.lib.sasb200_mlp_pack(*[w.data_ptr() for w in self.Wb],
                                               self.img.data_ptr(), self.stream.cuda_stream),
                     "mlp_pack")
         self._check(self.lib.sasb200_mlp_pack_t(*[w.data_ptr() for w in self.WTb[1:]],
                                                 self.img_t.data_ptr(), self.stream.cuda_stream),
                     "mlp_pack_t")
-        self._packed = key
 
     def infer(self, x, x_lo, n, blocks=0):
         """Inference only: out[n_pad] for features x + x_lo through the
@@ -217,14 +225,17 @@ class MLP:
     def gradients(self, x, x_lo, y, n):
         """Loss and gradients of one batch, all on self.stream: returns
         (loss, dW split partials [4], db [4], dw_out, db_out)."""
+        self._scratch(x.shape[0])
+        self._pack()
+        return self._gradient_kernels(x, x_lo, y, n)
+
+    def _gradient_kernels(self, x, x_lo, y, n):
         torch = self.torch
         n_pad = x.shape[0]
-        self._scratch(n_pad)
         st = self.stream.cuda_stream
         lib = self.lib
         # forward with the z/h planes and backward through the pipelined
         # persistent kernels (weights streamed from the packed images)
-        self._pack()
         self._check(lib.sasb200_mlp_infer(
             n, n_pad, x.data_ptr(), x_lo.data_ptr(), self.img.data_ptr(), self._ptrs(self.b),
             self.w_out.data_ptr(), self.b_out.data_ptr(), self.out.data_ptr(),
@@ -291,6 +302,16 @@ class MLP:
         with self.torch.cuda.stream(self.stream):
             dW = [g.view(self.splits, -1).sum(0) for g in dW]
             return [loss.reshape(1).clone()] + dW + [g.clone() for g in db + [gw, gbo]]
+
+    def capture_training(self, x_all, x_lo_all, y_all, batch, lr, total, step0, warmup=200,
+                         b1=0.9, b2=0.999, eps=1e-8):
+        """:class:`TrainingGraph` of one whole training step on `batch` rows
+        of (x_all, x_lo_all, y_all) chosen by an index buffer, with the
+        learning rate schedule of :meth:`Surrogate._train` (lr, total steps,
+        linear warm-up over `warmup` steps, cosine decay) advancing on the
+        device from schedule step `step0`."""
+        return TrainingGraph(self, x_all, x_lo_all, y_all, batch, lr, total, step0, warmup,
+                             b1, b2, eps)
 
     def apply_gradients(self, grads, lr, splits, b1=0.9, b2=0.999, eps=1e-8):
         """Adam update from [dW_1..dW_4 (each `splits` partials), db_1..db_4,
@@ -477,6 +498,68 @@ def gate_thresholds(r, err, tols, alpha):
     return np.maximum.accumulate(np.array(out, dtype=float))
 
 
+class TrainingGraph:
+    """One training step of an :class:`MLP` captured as a CUDA graph: the
+    batch gather (rows named by ``idx``), the weight images, forward,
+    loss, backward, weight gradients, the learning-rate schedule and Adam
+    for every parameter; the schedule's counters live on the device, so a
+    replay needs only the new row indices.  Launching the ~30 kernels of a
+    step from Python costs more host time than their device time at batch
+    8192; a replay costs one graph launch."""
+
+    def __init__(self, net, x_all, x_lo_all, y_all, batch, lr, total, step0, warmup,
+                 b1, b2, eps):
+        torch = net.torch
+        self.net = net
+        dev = net.device
+        if batch % TM:
+            raise ValueError("batch must be a multiple of %d" % TM)
+        self.batch = batch
+        self.idx = torch.zeros(batch, dtype=torch.int64, device=dev)
+        self.counters = torch.tensor([int(step0), int(net.step_count)], dtype=torch.int32,
+                                     device=dev)
+        self.sched = torch.zeros(4, dtype=torch.float32, device=dev)
+        self.xb = torch.empty((batch, x_all.shape[1]), dtype=x_all.dtype, device=dev)
+        self.xlb = torch.empty_like(self.xb)
+        self.yb = torch.empty(batch, dtype=y_all.dtype, device=dev)
+        net._scratch(batch)
+        lib, st = net.lib, net.stream.cuda_stream
+        net.stream.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph, stream=net.stream):
+            torch.index_select(x_all, 0, self.idx, out=self.xb)
+            torch.index_select(x_lo_all, 0, self.idx, out=self.xlb)
+            torch.index_select(y_all, 0, self.idx, out=self.yb)
+            net._check(lib.sasb200_lr_schedule(self.counters.data_ptr(), self.sched.data_ptr(),
+                                               int(total), int(warmup), float(lr), b1, b2, st),
+                       "lr_schedule")
+            net._pack_kernels()
+            self.loss, dW, db, gw, gbo = net._gradient_kernels(self.xb, self.xlb, self.yb, batch)
+            for l in range(4):
+                nb = NIN if l == 0 else HID
+                net._check(lib.sasb200_adam_sched(
+                    HID*nb, net.splits, dW[l].data_ptr(), net.W[l].data_ptr(),
+                    net.m[l].data_ptr(), net.v[l].data_ptr(), self.sched.data_ptr(), b1, b2, eps,
+                    net.Wb[l].data_ptr(), net.WTb[l].data_ptr(), HID, nb, st), "adam")
+            for k, g in enumerate(db + [gw, gbo]):
+                p = net.params[4 + k]
+                net._check(lib.sasb200_adam_sched(
+                    p.numel(), 1, g.data_ptr(), p.data_ptr(), net.m[4 + k].data_ptr(),
+                    net.v[4 + k].data_ptr(), self.sched.data_ptr(), b1, b2, eps, None, None,
+                    0, 0, st), "adam")
+
+    def step(self, idx):
+        """One training step on rows `idx` (int64 device tensor of `batch`
+        entries); returns the loss (a device scalar, overwritten by the
+        next step)."""
+        net = self.net
+        with net.torch.cuda.stream(net.stream):
+            self.idx.copy_(idx)
+            self.graph.replay()
+        net.step_count += 1
+        return self.loss
+
+
 class Surrogate:
     """Trained network, its error gate, target scalings and the gate's
     calibrated thresholds."""
@@ -542,24 +625,36 @@ class Surrogate:
         total = epochs*steps
         step = 0
         losses = []
+        # on one GPU the first step runs eagerly (every kernel loaded), the
+        # rest replay a CUDA graph of the step with the same schedule
+        graph = None
+        use_graph = nranks == 1 and (batch//nranks) % TM == 0
         for ep in range(epochs):
             perm = torch.as_tensor(rng.permutation(n), device=net.device)
             for s in range(steps):
                 lo, hi = batch_slice(s*batch, batch, rank, nranks)
                 idx = perm[lo:hi]
+                if graph is not None:
+                    loss = graph.step(idx)
+                    step += 1
+                    continue
                 with torch.cuda.stream(net.stream):
                     xb = x_all.index_select(0, idx)
                     xlb = xlo_all.index_select(0, idx)
                     tb = t_all.index_select(0, idx)
                 # cosine decay with a short warm-up
                 frac = step/total
-                rate = lr*min(1.0, (step + 1)/200)*0.5*(1 + math.cos(math.pi*frac))
+                rate = lr*min(1.0, (step + 1)/WARMUP_STEPS)*0.5*(1 + math.cos(math.pi*frac))
                 loss = net.train_step(xb, xlb, tb, hi - lo, rate, reduce=reduce)
                 step += 1
+                if use_graph and step < total:
+                    graph = net.capture_training(x_all, xlo_all, t_all, hi - lo, lr, total, step,
+                                                 warmup=WARMUP_STEPS)
             net.stream.synchronize()
             losses.append(float(loss.item())*scale**2)
             if log:
                 log("%s epoch %d loss %.3e" % (what, ep, losses[-1]))
+        graph = None
         if net.errors():
             raise RuntimeError("tensor-core kernel reported a timeout")
         return losses

@@ -331,3 +331,50 @@ def test_tc_data_parallel_replicas(cuda):
         assert torch.equal(p, q)
     for p, q in zip(a.Wb + a.WTb, b.Wb + b.WTb):
         assert torch.equal(p, q)
+
+
+@pytest.mark.gpu
+def test_training_graph_replays_the_eager_steps(cuda):
+    """A training step captured as a CUDA graph (batch gather by index
+    buffer, learning-rate schedule and Adam bias corrections advanced on the
+    device) updates the weights as the eager steps with the host-computed
+    schedule do."""
+    import math
+    import torch
+    from sasmodels_b200.surrogate import MLP, WARMUP_STEPS
+    rng = np.random.default_rng(21)
+    B, n, total, lr = 1024, 1024*6, 7, 3e-3
+    x = torch.as_tensor(mlp_ref.bf16(np.c_[rng.uniform(-1, 1, (n, 7)), np.zeros((n, 9))]),
+                        dtype=torch.bfloat16, device="cuda")
+    xlo = torch.zeros_like(x)
+    y = torch.as_tensor(rng.normal(0, 1, n), dtype=torch.float32, device="cuda")
+    idx = [torch.as_tensor(rng.permutation(n)[:B], device="cuda") for _ in range(total)]
+    eager, graphed = MLP(seed=4), MLP(seed=4)
+    losses_e, losses_g = [], []
+    for s in range(total):
+        rate = lr*min(1.0, (s + 1)/WARMUP_STEPS)*0.5*(1 + math.cos(math.pi*s/total))
+        with torch.cuda.stream(eager.stream):
+            xb, xlb, yb = x.index_select(0, idx[s]), xlo.index_select(0, idx[s]), y.index_select(0, idx[s])
+        losses_e.append(float(eager.train_step(xb, xlb, yb, B, rate).item()))
+    rate0 = lr*min(1.0, 1/WARMUP_STEPS)
+    with torch.cuda.stream(graphed.stream):
+        xb, xlb, yb = x.index_select(0, idx[0]), xlo.index_select(0, idx[0]), y.index_select(0, idx[0])
+    losses_g.append(float(graphed.train_step(xb, xlb, yb, B, rate0).item()))
+    g = graphed.capture_training(x, xlo, y, B, lr, total, 1, warmup=WARMUP_STEPS)
+    for s in range(1, total):
+        loss = g.step(idx[s])
+        graphed.stream.synchronize()
+        losses_g.append(float(loss.item()))
+    eager.stream.synchronize()
+    assert eager.errors() == 0 and graphed.errors() == 0
+    assert graphed.step_count == eager.step_count == total
+    np.testing.assert_allclose(losses_g, losses_e, rtol=1e-5)
+    for a, b in zip(graphed.params, eager.params):
+        a, b = a.cpu().numpy(), b.cpu().numpy()
+        assert np.abs(a - b).max() <= 1e-5*max(np.abs(b).max(), 1e-3)
+    # the weight images of inference are refreshed after graph steps
+    out_g = graphed.serve(x[:B], xlo[:B], B)
+    out_e = eager.serve(x[:B], xlo[:B], B)
+    graphed.stream.synchronize()
+    eager.stream.synchronize()
+    np.testing.assert_allclose(out_g.cpu().numpy(), out_e.cpu().numpy(), rtol=1e-4, atol=1e-5)
