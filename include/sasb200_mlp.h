@@ -102,6 +102,22 @@ int32_t sasb200_adam_sched(int32_t size, int32_t splits, const float *grad, floa
 int32_t sasb200_lr_schedule(int32_t *counters, float *sched, int32_t total, int32_t warmup,
                             float lr0, float b1, float b2, void *stream);
 
+/* all n (<= 16) parameter tensors in one launch: host arrays of n entries
+ * (device pointers; w[k], wt[k] may be NULL), the update of sasb200_adam_sched */
+int32_t sasb200_adam_multi(int32_t n, const int32_t *sizes, const int32_t *splits,
+                           const float *const *grads, float *const *p, float *const *m,
+                           float *const *v, void *const *w, void *const *wt, const int32_t *rows,
+                           const int32_t *cols, const float *sched, float b1, float b2, float eps,
+                           void *stream);
+
+/* out[c] = sum over r of M[r][c] (times v[r] when v is non-NULL) for a
+ * row-major bf16 [rows x cols] matrix, in a fixed order: partial sums of
+ * 64-row blocks into part (sasb200_col_sum_parts(rows) x cols floats), then
+ * each column's partials in block order. */
+int32_t sasb200_col_sums(int32_t rows, int32_t cols, const void *M, const float *v, float *part,
+                         float *out, void *stream);
+int32_t sasb200_col_sum_parts(int32_t rows);
+
 /* libsasb200_peaks.so: dependent-chain throughput probes (FP64 FMA, FP32
  * FMA, MUFU sine) whose measured rates are the roofline peaks of the
  * FP64 and FP32-compensated kernels. */

@@ -455,6 +455,35 @@ __global__ void row_dot(int rows, int cols, const __nv_bfloat16 *__restrict__ M,
     if (lane == 0) out[r] = s;
 }
 
+// Column sums of a row-major [rows x cols] bf16 matrix, each row weighted
+// by v[row] when v is given (the bias gradients from the dZ planes, the
+// output-layer gradient from the last h plane with v = dout).  Pass 1: one
+// thread per column sums CS_ROWS consecutive rows (coalesced row reads,
+// rows/CS_ROWS blocks); pass 2 adds each column's partials in block order,
+// so the result does not depend on scheduling.
+constexpr int CS_ROWS = 64;
+__global__ void col_sum_partial(int rows, int cols, const __nv_bfloat16 *__restrict__ M,
+                                const float *__restrict__ v, float *__restrict__ part)
+{
+    const int c = blockIdx.y*blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    const int r0 = blockIdx.x*CS_ROWS, r1 = min(rows, r0 + CS_ROWS);
+    float s = 0.0f;
+    for (int r = r0; r < r1; ++r)
+        s = fmaf(__bfloat162float(M[(size_t)r*cols + c]), v ? v[r] : 1.0f, s);
+    part[(size_t)blockIdx.x*cols + c] = s;
+}
+
+__global__ void col_sum_final(int nparts, int cols, const float *__restrict__ part,
+                              float *__restrict__ out)
+{
+    const int c = blockIdx.x*blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    float s = 0.0f;
+    for (int b = 0; b < nparts; ++b) s += part[(size_t)b*cols + c];
+    out[c] = s;
+}
+
 // Gradient of the mean loss over the first n rows (0 on padding) and the
 // per-row loss: squared error for delta <= 0, else Huber with threshold
 // delta (quadratic inside, linear outside), which keeps the few points
@@ -480,6 +509,31 @@ __global__ void loss_grad(int n, int n_pad, const float *__restrict__ out,
 
 // Adam on one FP32 master tensor; grad = sum of `splits` partial gradients.
 // Writes the BF16 copy (and its transpose if wt != nullptr, rows x cols).
+// Adam update of element i: the gradient summed over its `splits` split-K
+// partials, moments, parameter, and its bf16 copies (w; wt transposed).
+__device__ __forceinline__ void adam_element(int i, int size, int splits,
+                                             const float *__restrict__ grad,
+                                             float *__restrict__ p, float *__restrict__ m,
+                                             float *__restrict__ v, float lr, float b1, float b2,
+                                             float eps, float bc1, float bc2,
+                                             __nv_bfloat16 *__restrict__ w,
+                                             __nv_bfloat16 *__restrict__ wt, int rows, int cols)
+{
+    float g = 0.0f;
+    for (int s = 0; s < splits; ++s) g += grad[(size_t)s*size + i];
+    const float mi = b1*m[i] + (1.0f - b1)*g;
+    const float vi = b2*v[i] + (1.0f - b2)*g*g;
+    m[i] = mi;
+    v[i] = vi;
+    const float pi = p[i] - lr*(mi/bc1)/(sqrtf(vi/bc2) + eps);
+    p[i] = pi;
+    if (w) w[i] = __float2bfloat16_rn(pi);
+    if (wt) {
+        const int r = i/cols, c = i % cols;
+        wt[(size_t)c*rows + r] = __float2bfloat16_rn(pi);
+    }
+}
+
 // sched (optional, device): {lr, bc1, bc2} of this step, written by
 // lr_schedule; replaces the by-value lr, bc1, bc2 (a CUDA graph of a
 // training step then replays with the schedule advancing on the device).
@@ -496,19 +550,30 @@ __global__ void adam_step(int size, int splits, const float *__restrict__ grad, 
         bc1 = sched[1];
         bc2 = sched[2];
     }
-    float g = 0.0f;
-    for (int s = 0; s < splits; ++s) g += grad[(size_t)s*size + i];
-    const float mi = b1*m[i] + (1.0f - b1)*g;
-    const float vi = b2*v[i] + (1.0f - b2)*g*g;
-    m[i] = mi;
-    v[i] = vi;
-    const float pi = p[i] - lr*(mi/bc1)/(sqrtf(vi/bc2) + eps);
-    p[i] = pi;
-    if (w) w[i] = __float2bfloat16_rn(pi);
-    if (wt) {
-        const int r = i/cols, c = i % cols;
-        wt[(size_t)c*rows + r] = __float2bfloat16_rn(pi);
-    }
+    adam_element(i, size, splits, grad, p, m, v, lr, b1, b2, eps, bc1, bc2, w, wt, rows, cols);
+}
+
+// Every parameter tensor of the network in one launch (blockIdx.y = tensor),
+// the update of adam_step with lr and the bias corrections from sched.
+constexpr int ADAM_MAX_TENSORS = 16;
+struct AdamTensors {
+    int n;
+    int size[ADAM_MAX_TENSORS], splits[ADAM_MAX_TENSORS];
+    int rows[ADAM_MAX_TENSORS], cols[ADAM_MAX_TENSORS];
+    const float *grad[ADAM_MAX_TENSORS];
+    float *p[ADAM_MAX_TENSORS], *m[ADAM_MAX_TENSORS], *v[ADAM_MAX_TENSORS];
+    __nv_bfloat16 *w[ADAM_MAX_TENSORS], *wt[ADAM_MAX_TENSORS];
+};
+
+__global__ void adam_multi(AdamTensors T, float b1, float b2, float eps,
+                           const float *__restrict__ sched)
+{
+    const int k = blockIdx.y;
+    if (k >= T.n) return;
+    const int i = blockIdx.x*blockDim.x + threadIdx.x;
+    if (i >= T.size[k]) return;
+    adam_element(i, T.size[k], T.splits[k], T.grad[k], T.p[k], T.m[k], T.v[k], sched[0], b1, b2,
+                 eps, sched[1], sched[2], T.w[k], T.wt[k], T.rows[k], T.cols[k]);
 }
 
 // One training step's learning rate and Adam bias corrections from two
@@ -1621,6 +1686,54 @@ int32_t sasb200_adam_sched(int32_t size, int32_t splits, const float *grad, floa
         size, splits, grad, p, m, v, 0.0f, b1, b2, eps, 1.0f, 1.0f,
         static_cast<__nv_bfloat16 *>(w), static_cast<__nv_bfloat16 *>(wt), rows, cols, sched);
     return status("adam_step");
+}
+
+int32_t sasb200_adam_multi(int32_t n, const int32_t *sizes, const int32_t *splits,
+                           const float *const *grads, float *const *p, float *const *m,
+                           float *const *v, void *const *w, void *const *wt, const int32_t *rows,
+                           const int32_t *cols, const float *sched, float b1, float b2, float eps,
+                           void *stream)
+{
+    if (n <= 0 || n > ADAM_MAX_TENSORS || !sizes || !splits || !grads || !p || !m || !v || !w
+        || !wt || !rows || !cols || !sched)
+        return -1;
+    AdamTensors T;
+    T.n = n;
+    int most = 0;
+    for (int k = 0; k < n; ++k) {
+        if (sizes[k] <= 0 || splits[k] <= 0 || !grads[k] || !p[k] || !m[k] || !v[k]) return -1;
+        if (wt[k] && rows[k]*cols[k] != sizes[k]) return -1;
+        T.size[k] = sizes[k];
+        T.splits[k] = splits[k];
+        T.rows[k] = rows[k];
+        T.cols[k] = cols[k];
+        T.grad[k] = grads[k];
+        T.p[k] = p[k];
+        T.m[k] = m[k];
+        T.v[k] = v[k];
+        T.w[k] = static_cast<__nv_bfloat16 *>(w[k]);
+        T.wt[k] = static_cast<__nv_bfloat16 *>(wt[k]);
+        most = sizes[k] > most ? sizes[k] : most;
+    }
+    adam_multi<<<dim3((most + 255)/256, n), 256, 0, (cudaStream_t)stream>>>(T, b1, b2, eps, sched);
+    return status("adam_multi");
+}
+
+int32_t sasb200_col_sums(int32_t rows, int32_t cols, const void *M, const float *v, float *part,
+                         float *out, void *stream)
+{
+    if (rows < 0 || cols <= 0 || !M || !part || !out) return -1;
+    const int nparts = rows > 0 ? (rows + CS_ROWS - 1)/CS_ROWS : 0;
+    if (nparts)
+        col_sum_partial<<<dim3(nparts, (cols + 255)/256), 256, 0, (cudaStream_t)stream>>>(
+            rows, cols, static_cast<const __nv_bfloat16 *>(M), v, part);
+    col_sum_final<<<(cols + 255)/256, 256, 0, (cudaStream_t)stream>>>(nparts, cols, part, out);
+    return status("col_sums");
+}
+
+int32_t sasb200_col_sum_parts(int32_t rows)
+{
+    return rows > 0 ? (rows + CS_ROWS - 1)/CS_ROWS : 0;
 }
 
 int32_t sasb200_lr_schedule(int32_t *counters, float *sched, int32_t total, int32_t warmup,

@@ -60,6 +60,9 @@ def _lib():
     lib.sasb200_adam.argtypes = [I, I, P, P, P, P, F, F, F, F, I, P, P, I, I, P]
     lib.sasb200_adam_sched.argtypes = [I, I, P, P, P, P, P, F, F, F, P, P, I, I, P]
     lib.sasb200_lr_schedule.argtypes = [P, P, I, I, F, F, F, P]
+    lib.sasb200_adam_multi.argtypes = [I, P, P, P, P, P, P, P, P, P, P, P, F, F, F, P]
+    lib.sasb200_col_sums.argtypes = [I, I, P, P, P, P, P]
+    lib.sasb200_col_sum_parts.argtypes = [I]
     lib.sasb200_mlp_features.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P]
     lib.sasb200_mlp_pack.argtypes = [P, P, P, P, P, P]
     lib.sasb200_mlp_infer.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P, I, P]
@@ -71,7 +74,8 @@ def _lib():
                  "sasb200_adam", "sasb200_mlp_features", "sasb200_mlp_pack",
                  "sasb200_mlp_infer", "sasb200_mlp_serve", "sasb200_mlp_image_bytes",
                  "sasb200_mlp_pack_t", "sasb200_mlp_image_t_bytes", "sasb200_mlp_backward_p",
-                 "sasb200_adam_sched", "sasb200_lr_schedule"):
+                 "sasb200_adam_sched", "sasb200_lr_schedule", "sasb200_adam_multi",
+                 "sasb200_col_sums", "sasb200_col_sum_parts"):
         getattr(lib, name).restype = I
     lib.sasb200_mlp_last_error.restype = ct.c_char_p
     return lib
@@ -152,6 +156,7 @@ class MLP:
         self.out = torch.empty(n_pad, **f32)
         self.dout = torch.empty(n_pad, **f32)
         self.sq = torch.empty(n_pad, **f32)
+        self.cs_part = torch.empty(self.lib.sasb200_col_sum_parts(n_pad)*HID, **f32)
         self.splits = 32     # split-K of the weight gradients: 64+ CTAs at batch 8192
         self.gW = [torch.empty(self.splits*HID*(NIN if l == 0 else HID), **f32)
                    for l in range(4)]
@@ -264,13 +269,15 @@ class MLP:
                                             self.t_b.data_ptr(), self.splits,
                                             self.gW[l].data_ptr(), self.err.data_ptr(), st),
                         "gemm_nt")
-            self._check(lib.sasb200_row_dot(HID, n_pad, self.t_a.data_ptr(), None,
-                                            self.gb[l].data_ptr(), st), "row_dot")
+            # bias gradient: column sums of the dZ plane (zero on padding rows)
+            self._check(lib.sasb200_col_sums(n_pad, HID, dz.data_ptr(), None,
+                                             self.cs_part.data_ptr(), self.gb[l].data_ptr(), st),
+                        "col_sums")
+        # output weights: columns of the last h plane weighted by dout
         h3 = self.h_save[3*plane:4*plane]
-        self._check(lib.sasb200_transpose_bf16(n_pad, HID, h3.data_ptr(), self.t_b.data_ptr(), st),
-                    "transpose")
-        self._check(lib.sasb200_row_dot(HID, n_pad, self.t_b.data_ptr(), self.dout.data_ptr(),
-                                        self.gw.data_ptr(), st), "row_dot")
+        self._check(lib.sasb200_col_sums(n_pad, HID, h3.data_ptr(), self.dout.data_ptr(),
+                                         self.cs_part.data_ptr(), self.gw.data_ptr(), st),
+                    "col_sums")
         with torch.cuda.stream(self.stream):
             self.gbo.copy_(self.dout[:n_pad].sum().reshape(1))
             loss = self.sq[:n].mean()
@@ -535,18 +542,20 @@ class TrainingGraph:
                        "lr_schedule")
             net._pack_kernels()
             self.loss, dW, db, gw, gbo = net._gradient_kernels(self.xb, self.xlb, self.yb, batch)
-            for l in range(4):
-                nb = NIN if l == 0 else HID
-                net._check(lib.sasb200_adam_sched(
-                    HID*nb, net.splits, dW[l].data_ptr(), net.W[l].data_ptr(),
-                    net.m[l].data_ptr(), net.v[l].data_ptr(), self.sched.data_ptr(), b1, b2, eps,
-                    net.Wb[l].data_ptr(), net.WTb[l].data_ptr(), HID, nb, st), "adam")
-            for k, g in enumerate(db + [gw, gbo]):
-                p = net.params[4 + k]
-                net._check(lib.sasb200_adam_sched(
-                    p.numel(), 1, g.data_ptr(), p.data_ptr(), net.m[4 + k].data_ptr(),
-                    net.v[4 + k].data_ptr(), self.sched.data_ptr(), b1, b2, eps, None, None,
-                    0, 0, st), "adam")
+            grads = dW + db + [gw, gbo]
+            nt = len(net.params)
+            I32, VP = ct.c_int32*nt, ct.c_void_p*nt
+            sizes = [p.numel() for p in net.params]
+            splits = [net.splits if k < 4 else 1 for k in range(nt)]
+            shape = [(HID, NIN if k == 0 else HID) if k < 4 else (0, 0) for k in range(nt)]
+            net._check(lib.sasb200_adam_multi(
+                nt, I32(*sizes), I32(*splits), VP(*[g.data_ptr() for g in grads]),
+                VP(*[p.data_ptr() for p in net.params]), VP(*[m.data_ptr() for m in net.m]),
+                VP(*[v.data_ptr() for v in net.v]),
+                VP(*[net.Wb[k].data_ptr() if k < 4 else None for k in range(nt)]),
+                VP(*[net.WTb[k].data_ptr() if k < 4 else None for k in range(nt)]),
+                I32(*[r for r, _ in shape]), I32(*[c for _, c in shape]),
+                self.sched.data_ptr(), b1, b2, eps, st), "adam_multi")
 
     def step(self, idx):
         """One training step on rows `idx` (int64 device tensor of `batch`

@@ -378,3 +378,29 @@ def test_training_graph_replays_the_eager_steps(cuda):
     graphed.stream.synchronize()
     eager.stream.synchronize()
     np.testing.assert_allclose(out_g.cpu().numpy(), out_e.cpu().numpy(), rtol=1e-4, atol=1e-5)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rows", [1, 63, 1000, 8192])
+def test_col_sums(cuda, rows):
+    """Column sums of a bf16 matrix (plain and row-weighted), the bias and
+    output-layer gradients of training, against float64 sums."""
+    import torch
+    from sasmodels_b200.surrogate import _lib
+    lib = _lib()
+    rng = np.random.default_rng(rows)
+    M = mlp_ref.bf16(rng.normal(0, 1, (rows, 256)))
+    v = rng.normal(0, 1, rows).astype(np.float32)
+    Md = torch.as_tensor(M, dtype=torch.bfloat16, device="cuda")
+    vd = torch.as_tensor(v, device="cuda")
+    part = torch.empty(lib.sasb200_col_sum_parts(rows)*256, dtype=torch.float32, device="cuda")
+    out = torch.empty(256, dtype=torch.float32, device="cuda")
+    for weights in (None, vd):
+        st = torch.cuda.current_stream().cuda_stream
+        assert lib.sasb200_col_sums(rows, 256, Md.data_ptr(),
+                                    weights.data_ptr() if weights is not None else None,
+                                    part.data_ptr(), out.data_ptr(), st) == 0
+        torch.cuda.synchronize()
+        want = (M*(v[:, None].astype(np.float64) if weights is not None else 1.0)).sum(axis=0)
+        scale = np.abs(M).sum(axis=0)*(np.abs(v).max() if weights is not None else 1.0)
+        assert np.all(np.abs(out.cpu().numpy() - want) <= 1e-5*scale)
