@@ -363,6 +363,10 @@ def reference_surrogate(n_sets=16, nq=1000, seed=2):
 def run_reference(args, world, rank):
     if rank != 0:
         return
+    if args.config == "mlp":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "sasmodels has no learned surrogate network"}), flush=True)
+        return
     if args.config in ("population", "surrogate"):
         fn = reference_population if args.config == "population" else reference_surrogate
         unit = "param-sets/s" if args.config == "population" else "samples/s"
@@ -939,6 +943,9 @@ def surrogate_extra(dev, n_train_sets=50000, epochs=32, gate_epochs=16, n_holdou
 #: The kernels issue the hidden layers twice (the compensated hi and lo
 #: activations), which this algorithmic count leaves out.
 MLP_FLOPS_PER_ROW = 2*(16*256 + 3*256*256 + 256)
+#: DRAM bytes (read + write) of one mlp_serve launch over 4,000,000 rows, from
+#: ncu (profiles/mlp_surrogate.md): the features in and the outputs out
+MLP_SERVE_TRAFFIC = 278.5e6
 
 
 def bf16_peak():
@@ -1152,6 +1159,64 @@ def run_population_split(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_mlp(args, world, rank, local):
+    """The surrogate network's kernels alone, random weights: one inference
+    launch over 4,000,000 rows through the overlapped serving kernel (the
+    line's value) and the pipelined training forward, and one training step
+    at batch 8192 replayed from its CUDA graph."""
+    if rank != 0:
+        return
+    import torch
+    from sasmodels_b200.surrogate import MLP
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    net = MLP(seed=3, device=dev)
+    reps = max(args.steps, 5)
+    times = mlp_kernel_times(net, reps=reps)
+    serve = times["mlp_serve"]
+    # training: one eager step loads the kernels, then the captured step
+    B, nrows = 8192, 8192*64
+    g = torch.Generator(device=dev).manual_seed(7)
+    x = (0.5*torch.randn(nrows, 16, device=dev, generator=g)).to(torch.bfloat16)
+    x_lo = torch.zeros_like(x)
+    y = torch.randn(nrows, device=dev, generator=g)
+    perm = torch.randperm(nrows, device=dev, generator=g)
+    net.train_step(x[:B], x_lo[:B], y[:B], B, 1e-4)
+    graph = net.capture_training(x, x_lo, y, B, 1e-3, 100000, 1)
+    for i in range(args.warmup + 10):
+        graph.step(perm[(i % 64)*B:(i % 64 + 1)*B])
+    n_steps = 200
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(net.stream)
+    for i in range(n_steps):
+        graph.step(perm[(i % 64)*B:(i % 64 + 1)*B])
+    ev[1].record(net.stream)
+    ev[1].synchronize()
+    if net.errors():
+        raise RuntimeError("surrogate kernel pipeline error %d" % net.errors())
+    peak, source = bf16_peak()
+    line = {
+        "metric": "surrogate network inference rows/s (mlp_serve)",
+        "value": serve["rows_per_s"], "unit": "rows/s", "n_gpus": 1, "steps": reps,
+        "warmup": 3, "ms_per_step": serve["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16 (compensated activations), f32 accumulate",
+        "data": "synthetic (random weights and features)",
+        "config": {"workload": "16 -> 4 x 256 SiLU -> 1 network, 4,000,000 rows per launch "
+                               "(features 2 x 128 MB, above L2)"},
+        "roofline": {"bound": "tensor", "unit": "TFLOP/s",
+                     "achieved": serve["algorithmic_tflops"], "peak": peak,
+                     "peak_source": source, "frac": serve["frac"],
+                     "numerator": "MLP_FLOPS_PER_ROW (0.402 MFLOP) x rows; the hi and lo "
+                                  "activation halves double the issued MMAs",
+                     "traffic": MLP_SERVE_TRAFFIC},
+        "mlp_kernels": times,
+        "training_step": {"batch": B, "ms": ev[0].elapsed_time(ev[1])/n_steps,
+                          "what": "one replay of the captured training step (gather, schedule, "
+                                  "forward with planes, backward, gradients, Adam)"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_surrogate(args, world, rank, local):
     """Learned surrogate: train on plain-kernel data, judge on held-out sets,
     time the network with automatic fallback against the plain FP64 path."""
@@ -1187,7 +1252,8 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="cylinder2d",
-                    choices=["cylinder2d", "sphere1d", "magnetic", "surrogate", "population"])
+                    choices=["cylinder2d", "sphere1d", "magnetic", "surrogate", "population",
+                             "mlp"])
     ap.add_argument("--pop-stride", type=int, default=7,
                     help="population config: evaluate every n-th of the 4096 sets")
     ap.add_argument("--surrogate-holdout", type=int, default=3000,
@@ -1218,6 +1284,8 @@ def main(argv=None):
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.config == "mlp":
+            run_mlp(args, world, rank, local)
         elif args.config == "surrogate":
             run_surrogate(args, world, rank, local)
         elif args.config == "population":
