@@ -113,7 +113,7 @@ int32_t sasb200_adam_multi(int32_t n, const int32_t *sizes, const int32_t *split
 /* out[c] = sum over r of M[r][c] (times v[r] when v is non-NULL) for a
  * row-major bf16 [rows x cols] matrix, in a fixed order: partial sums of
  * 64-row blocks into part (sasb200_col_sum_parts(rows) x cols floats), then
- * each column's partials in block order. */
+ * each column's partials combined in a fixed order (one warp per column). */
 int32_t sasb200_col_sums(int32_t rows, int32_t cols, const void *M, const float *v, float *part,
                          float *out, void *stream);
 int32_t sasb200_col_sum_parts(int32_t rows);

@@ -458,9 +458,11 @@ __global__ void row_dot(int rows, int cols, const __nv_bfloat16 *__restrict__ M,
 // Column sums of a row-major [rows x cols] bf16 matrix, each row weighted
 // by v[row] when v is given (the bias gradients from the dZ planes, the
 // output-layer gradient from the last h plane with v = dout).  Pass 1: one
-// thread per column sums CS_ROWS consecutive rows (coalesced row reads,
-// rows/CS_ROWS blocks); pass 2 adds each column's partials in block order,
-// so the result does not depend on scheduling.
+// thread per column sums CS_ROWS consecutive rows (coalesced row reads, the
+// loads of a block of rows in flight together, rows/CS_ROWS blocks); pass
+// 2: one warp per column, lane j adding partials j, j + 32, ... in order and
+// the lanes combined by a butterfly, so the result does not depend on
+// scheduling.
 constexpr int CS_ROWS = 64;
 __global__ void col_sum_partial(int rows, int cols, const __nv_bfloat16 *__restrict__ M,
                                 const float *__restrict__ v, float *__restrict__ part)
@@ -469,19 +471,35 @@ __global__ void col_sum_partial(int rows, int cols, const __nv_bfloat16 *__restr
     if (c >= cols) return;
     const int r0 = blockIdx.x*CS_ROWS, r1 = min(rows, r0 + CS_ROWS);
     float s = 0.0f;
-    for (int r = r0; r < r1; ++r)
-        s = fmaf(__bfloat162float(M[(size_t)r*cols + c]), v ? v[r] : 1.0f, s);
+    if (r1 - r0 == CS_ROWS) {
+        float m[CS_ROWS/4];
+        #pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            #pragma unroll
+            for (int j = 0; j < CS_ROWS/4; ++j)
+                m[j] = __bfloat162float(M[(size_t)(r0 + q*(CS_ROWS/4) + j)*cols + c]);
+            #pragma unroll
+            for (int j = 0; j < CS_ROWS/4; ++j)
+                s = fmaf(m[j], v ? v[r0 + q*(CS_ROWS/4) + j] : 1.0f, s);
+        }
+    } else {
+        for (int r = r0; r < r1; ++r)
+            s = fmaf(__bfloat162float(M[(size_t)r*cols + c]), v ? v[r] : 1.0f, s);
+    }
     part[(size_t)blockIdx.x*cols + c] = s;
 }
 
 __global__ void col_sum_final(int nparts, int cols, const float *__restrict__ part,
                               float *__restrict__ out)
 {
-    const int c = blockIdx.x*blockDim.x + threadIdx.x;
+    const int c = blockIdx.x*(blockDim.x/32) + threadIdx.x/32;
+    const int lane = threadIdx.x & 31;
     if (c >= cols) return;
     float s = 0.0f;
-    for (int b = 0; b < nparts; ++b) s += part[(size_t)b*cols + c];
-    out[c] = s;
+    for (int b = lane; b < nparts; b += 32) s += part[(size_t)b*cols + c];
+    #pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) out[c] = s;
 }
 
 // Gradient of the mean loss over the first n rows (0 on padding) and the
@@ -1727,7 +1745,7 @@ int32_t sasb200_col_sums(int32_t rows, int32_t cols, const void *M, const float 
     if (nparts)
         col_sum_partial<<<dim3(nparts, (cols + 255)/256), 256, 0, (cudaStream_t)stream>>>(
             rows, cols, static_cast<const __nv_bfloat16 *>(M), v, part);
-    col_sum_final<<<(cols + 255)/256, 256, 0, (cudaStream_t)stream>>>(nparts, cols, part, out);
+    col_sum_final<<<(cols + 7)/8, 256, 0, (cudaStream_t)stream>>>(nparts, cols, part, out);
     return status("col_sums");
 }
 

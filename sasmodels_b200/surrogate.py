@@ -629,7 +629,10 @@ class Surrogate:
 
             def reduce(grads):
                 allreduce_mean(grads, group)
-        rng = np.random.default_rng(seed)
+        # the epochs' row orders come from a seeded generator on the device
+        # (every replica of a data-parallel run draws the same ones)
+        gen = torch.Generator(device=net.device)
+        gen.manual_seed(int(seed))
         steps = max(1, n//batch)
         total = epochs*steps
         step = 0
@@ -639,7 +642,7 @@ class Surrogate:
         graph = None
         use_graph = nranks == 1 and (batch//nranks) % TM == 0
         for ep in range(epochs):
-            perm = torch.as_tensor(rng.permutation(n), device=net.device)
+            perm = torch.randperm(n, device=net.device, generator=gen)
             for s in range(steps):
                 lo, hi = batch_slice(s*batch, batch, rank, nranks)
                 idx = perm[lo:hi]
