@@ -355,11 +355,15 @@ def test_training_graph_replays_the_eager_steps(cuda):
         rate = lr*min(1.0, (s + 1)/WARMUP_STEPS)*0.5*(1 + math.cos(math.pi*s/total))
         with torch.cuda.stream(eager.stream):
             xb, xlb, yb = x.index_select(0, idx[s]), xlo.index_select(0, idx[s]), y.index_select(0, idx[s])
-        losses_e.append(float(eager.train_step(xb, xlb, yb, B, rate).item()))
+        loss = eager.train_step(xb, xlb, yb, B, rate)
+        eager.stream.synchronize()          # the loss is computed on the net's stream
+        losses_e.append(float(loss.item()))
     rate0 = lr*min(1.0, 1/WARMUP_STEPS)
     with torch.cuda.stream(graphed.stream):
         xb, xlb, yb = x.index_select(0, idx[0]), xlo.index_select(0, idx[0]), y.index_select(0, idx[0])
-    losses_g.append(float(graphed.train_step(xb, xlb, yb, B, rate0).item()))
+    loss = graphed.train_step(xb, xlb, yb, B, rate0)
+    graphed.stream.synchronize()
+    losses_g.append(float(loss.item()))
     g = graphed.capture_training(x, xlo, y, B, lr, total, 1, warmup=WARMUP_STEPS)
     for s in range(1, total):
         loss = g.step(idx[s])
