@@ -96,8 +96,9 @@ SASB200_DECLARE_MODEL(cylinder)
  * The cylinder library's sasb200_cylinder_Iqxy runs a hand-rearranged FP64
  * form of the plugin's Iqac (cylinder.c:92-102, lib/sas_J1.c:107-153) with
  * the per-mesh-point work (contrast x volume, scale factor, weight, R, L/2,
- * rotation row) hoisted out of the q loop and fewer divisions in J1; within
- * 1e-12 of the reference DLL like every FP64 entry point.  The plugin's C as
+ * rotation row) hoisted out of the q loop, fewer divisions in J1 and those
+ * left taken as Newton reciprocals; within 1e-12 of the reference DLL like
+ * every FP64 entry point.  The plugin's C as
  * translated, without that rearrangement, stays exported under the prefix
  * cylinder_plugin (same arguments) for comparison.
  */
