@@ -121,6 +121,7 @@ def build_model(name, force=False, verbose=False, extra_flags=()):
                               + _read(os.path.join(CSRC, "sas_driver.cuh"))
                               + _read(os.path.join(CSRC, "sas_abi.cuh"))
                               + _read(os.path.join(CSRC, "sas_device.cuh"))
+                              + _read(os.path.join(CSRC, "fp64_recip.cuh"))
                               + _read(os.path.join(CSRC, "sas_noalloc.cuh"))
                               + "".join(_read(os.path.join(CSRC, h))
                                         for h in generate.HOISTED_MODELS.values())

@@ -19,6 +19,8 @@
 // once per (q, mesh point) and every channel only recombines them, with the
 // reference's operations in the reference's order (V b (contrast) as
 // (V b) contrast: the product V b is the same double in every channel).
+// 3 j1(x)/x is lib/sas_3j1x_x.c:46-57 restated with its two divisions of
+// the closed form as one Newton reciprocal of x (recip_nr, fp64_recip.cuh).
 // The non-magnetic variants are the plugin's as translated.
 
 struct SasModelHoisted : SasModel {
@@ -27,13 +29,27 @@ struct SasModelHoisted : SasModel {
     // sum over the five distinct channels c with chan_w[c] > 0 of
     // chan_w[c] * F^2(q; v with the slds of channel c); v = radius,
     // thickness, sld_core, sld_shell, sld_solvent
+    // 3 j1(x)/x: the reference's series below |x| = 0.1, above it
+    // 3 (sin x/x - cos x)/x^2 with r = 1/x as 3 (sin x r - cos x) r^2
+    __device__ static double sph_j1x3(double x)
+    {
+        if (fabs(x) < 0.1) {
+            const double x2 = x*x;
+            return 1.0 + x2*(-3./30. + x2*(3./840. + x2*(-3./45360.)));
+        }
+        double s, c;
+        sincos(x, &s, &c);
+        const double r = recip_nr(x);
+        return 3.0*(s*r - c)*(r*r);
+    }
+
     __device__ static double mag_channels(double q, const double *v, const double (*eff)[3],
                                           const double *chan_w)
     {
         const double radius = v[0], thickness = v[1];
-        const double vb_core = (M_4PI_3*cube(radius))*sas_3j1x_x(q*radius);
+        const double vb_core = (M_4PI_3*cube(radius))*sph_j1x3(q*radius);
         const double outer = radius + thickness;
-        const double vb_shell = (M_4PI_3*cube(outer))*sas_3j1x_x(q*outer);
+        const double vb_shell = (M_4PI_3*cube(outer))*sph_j1x3(q*outer);
         double F2 = 0.0;
         #pragma unroll
         for (int c = 0; c < 5; ++c) {

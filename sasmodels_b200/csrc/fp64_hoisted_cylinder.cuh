@@ -29,12 +29,10 @@
 //     evaluation divides once on x <= 5 and twice on x > 5 (the reference:
 //     three and five times);
 //   * those divisions are a multiplication by a reciprocal from Newton's
-//     method: the hardware's approximate reciprocal (rcp.approx.ftz.f64)
-//     refined by two iterations x <- x + x (1 - d x), each squaring the
-//     relative error, to within an ulp or two of 1/d.  Its arguments stay
-//     in the normal range: den is a positive polynomial value, x > 5 on the
-//     asymptotic branch, and |y| < 1e-100 counts as y = 0, where sin(y)/y
-//     already rounds to 1.
+//     method (recip_nr, fp64_recip.cuh), within an ulp or two of 1/d.  Its
+//     arguments stay in the normal range: den is a positive polynomial
+//     value, x > 5 on the asymptotic branch, and |y| < 1e-100 counts as
+//     y = 0, where sin(y)/y already rounds to 1.
 //
 // Each change moves a result by a few units in the last place; the mesh
 // sums of these non-negative terms stay within 1e-12 of the reference DLL
@@ -75,22 +73,6 @@ struct SasModelHoisted : SasModel {
 #endif
     }
 
-    // 1/d by two Newton iterations from the approximate reciprocal (d a
-    // normal double); exact division on the host
-    __device__ static double recip(double d)
-    {
-#ifdef __CUDA_ARCH__
-        double x;
-        asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(d));
-        double e = fma(-d, x, 1.0);
-        x = fma(x, e, x);
-        e = fma(-d, x, 1.0);
-        return fma(x, e, x);
-#else
-        return 1.0/d;
-#endif
-    }
-
     // 2 J1(x)/x as num/den, for x^2 = z (x = qab R >= 0; qab_sq = qab^2)
     __device__ static void j1x_parts(double z, double qab_sq, double R, double &num,
                                      double &den)
@@ -101,7 +83,7 @@ struct SasModelHoisted : SasModel {
             return;
         }
         const double ax = sqrt(qab_sq)*R;
-        const double inv = recip(ax);
+        const double inv = recip_nr(ax);
         const double w = 5.0*inv;
         const double zz = w*w;
         const double pp = polevl(zz, PPJ1, 6), pq = polevl(zz, PQJ1, 6);
@@ -135,7 +117,7 @@ struct SasModelHoisted : SasModel {
         // sin(y)/y folded into the same division (1 at y = 0)
         const double y = qc*halfL;
         const bool y0 = fabs(y) < 1.0e-100;
-        const double f = (num*(y0 ? 1.0 : sin(y)))*recip(den*(y0 ? 1.0 : y));
+        const double f = (num*(y0 ? 1.0 : sin(y)))*recip_nr(den*(y0 ? 1.0 : y));
         return A*(f*f);
     }
 };

@@ -20,6 +20,8 @@
 #include <cstdint>
 #include <cmath>
 
+#include "fp64_recip.cuh"
+
 #undef M_PI
 #undef M_PI_2
 #undef M_PI_4

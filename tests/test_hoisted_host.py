@@ -32,6 +32,7 @@ pytestmark = pytest.mark.skipif(SASMODELS is None or shutil.which("g++") is None
 PRELUDE = """
 #define FLOAT_SIZE 8
 #include "sas_host.h"
+#include "fp64_recip.cuh"
 #define __device__
 #define __forceinline__
 static inline double rsqrt(double x) { return 1.0/sqrt(x); }
