@@ -1048,7 +1048,7 @@ SASFLOPS = {
 #: per thread instruction) over the evaluations of the captured launch; the
 #: issued count includes the operations CUDA's sin, sqrt and division expand
 #: into, so it sits above the algorithmic count (profiles/iq_main_*.md).
-ISSUED_FP64_PER_EVAL = {"cylinder2d": 95.1, "magnetic": 197.3}
+ISSUED_FP64_PER_EVAL = {"cylinder2d": 95.1, "magnetic": 157.3}
 #: configurations whose kernel skips work the reference repeats, so that the
 #: algorithmic count divided by the kernel's time can exceed the peak
 ROOFLINE_NOTES = {
