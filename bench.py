@@ -504,12 +504,15 @@ def run_b200(args, world, rank, local):
                 I = multigpu.gather_blocks(torch.as_tensor(I)).cpu().numpy()
             return I
 
-        e2e_step()
-        # the setup's garbage is collected before the clock starts; the
-        # collector stays on while the steps are timed
-        gc.collect()
-        barrier()
+        # the clock sampler (an nvidia-smi process, costly to start) is
+        # started before the untimed warm-up step, and the setup's garbage is
+        # collected before the clock starts; the sampler and the collector
+        # both stay on while the steps are timed
         with ClockSampler(local, "_e2e") as e2e_clocks:
+            e2e_step()
+            gc.collect()
+            time.sleep(0.5)
+            barrier()
             t0 = time.perf_counter()
             for _ in range(args.steps):
                 e2e_step()

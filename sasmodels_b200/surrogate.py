@@ -948,22 +948,24 @@ def train_and_evaluate(n_train_sets=50000, nq=1000, epochs=10, n_holdout_sets=10
     # plain FP32c path for reference; one untimed call of each first
     plain_unit_iq({k: v[:8] for k, v in ev[0].items()}, ev[1][:8], S.net.device, "double")
     plain_unit_iq({k: v[:8] for k, v in ev[0].items()}, ev[1][:8], S.net.device, "float32c")
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    ev_iq = plain_unit_iq(ev[0], ev[1], S.net.device, "double")
-    torch.cuda.synchronize()
-    t_plain = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    plain_unit_iq(ev[0], ev[1], S.net.device, "float32c")
-    torch.cuda.synchronize()
-    t_plain32 = time.perf_counter() - t0
+    # every arm below is timed on the host clock as the mean of REPS calls,
+    # so that one stall of the host does not decide a ratio
+    REPS = 3
+
+    def timed(fn):
+        out, total = None, 0.0
+        for _ in range(REPS):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = fn()
+            torch.cuda.synchronize()
+            total += time.perf_counter() - t0
+        return out, total/REPS
+    ev_iq, t_plain = timed(lambda: plain_unit_iq(ev[0], ev[1], S.net.device, "double"))
+    _, t_plain32 = timed(lambda: plain_unit_iq(ev[0], ev[1], S.net.device, "float32c"))
     truth = np.log(np.concatenate(ev_iq)) + 2*np.log(np.abs(ev_cols["contrast"]))
     S.predict_log(ev_cols)            # warm
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    S.predict_log(ev_cols)
-    torch.cuda.synchronize()
-    t_net = time.perf_counter() - t0
+    _, t_net = timed(lambda: S.predict_log(ev_cols))
     logi, g = S._outputs(ev_cols)
     raw = np.abs(logi - truth)
     n = len(truth)
@@ -981,11 +983,7 @@ def train_and_evaluate(n_train_sets=50000, nq=1000, epochs=10, n_holdout_sets=10
     for t in sorted({tol, 0.05}):
         S.iq(ev_cols, tol=t)
     for t in sorted({tol, 0.05}):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        I, back = S.iq(ev_cols, tol=t)
-        torch.cuda.synchronize()
-        t_sur = time.perf_counter() - t0
+        (I, back), t_sur = timed(lambda: S.iq(ev_cols, tol=t))
         err = np.abs(np.log(I) - truth)
         report["operating_points"]["%g" % t] = dict(
             net_frac_within=float(np.mean(raw <= t)), fallback_frac=float(back.mean()),
