@@ -69,7 +69,7 @@ int32_t sasb200_mlp_backward_p(int32_t n, int32_t n_pad, const void *img_t, cons
  * (z_save, h_save: [4][n_pad x 256] bf16 each, or both NULL), backward
  * through the hidden layers (wt: transposed bf16 weights), weight
  * gradients as split-K partial GEMMs C[splits][M x nb] = A[M x K] B[nb x K]^T,
- * row sums / dots, Huber loss gradient, Adam (also refreshing the bf16
+ * Huber loss gradient, Adam (also refreshing the bf16
  * copies w and, if non-NULL, the transposed wt). */
 int32_t sasb200_mlp_forward(int32_t n, int32_t n_pad, const void *x, const void *x_lo,
                             const void *const *w, const float *const *b, const float *w_out,
@@ -83,27 +83,24 @@ int32_t sasb200_gemm_nt(int32_t M, int32_t nb, int32_t K, int32_t lda, int32_t l
                         void *stream);
 int32_t sasb200_transpose_bf16(int32_t rows, int32_t cols, const void *src, void *dst,
                                void *stream);
-int32_t sasb200_row_dot(int32_t rows, int32_t cols, const void *M, const float *v, float *out,
-                        void *stream);
 int32_t sasb200_loss_grad(int32_t n, int32_t n_pad, const float *out, const float *y,
                           float delta, float *dout, float *loss, void *stream);
 int32_t sasb200_adam(int32_t size, int32_t splits, const float *grad, float *p, float *m,
                      float *v, float lr, float b1, float b2, float eps, int32_t step, void *w,
                      void *wt, int32_t rows, int32_t cols, void *stream);
 
-/* the same Adam update with lr and the bias corrections read from the device
- * (sched = {lr, 1 - b1^t, 1 - b2^t}), and the kernel that writes them:
- * counters = {schedule step s, Adam step count t} (int32, device), lr = lr0
- * min(1, (s + 1)/warmup) (1 + cos(pi s/total))/2, then s and t advance by
- * one.  A CUDA graph of a whole training step replays with these. */
-int32_t sasb200_adam_sched(int32_t size, int32_t splits, const float *grad, float *p, float *m,
-                           float *v, const float *sched, float b1, float b2, float eps,
-                           void *w, void *wt, int32_t rows, int32_t cols, void *stream);
+/* the learning rate and Adam bias corrections of a training step, on the
+ * device: counters = {schedule step s, Adam step count t} (int32), sched =
+ * {lr, 1 - b1^t, 1 - b2^t} with lr = lr0 min(1, (s + 1)/warmup)
+ * (1 + cos(pi s/total))/2, then s and t advance by one.  A CUDA graph of a
+ * whole training step replays with these. */
 int32_t sasb200_lr_schedule(int32_t *counters, float *sched, int32_t total, int32_t warmup,
                             float lr0, float b1, float b2, void *stream);
 
-/* all n (<= 16) parameter tensors in one launch: host arrays of n entries
- * (device pointers; w[k], wt[k] may be NULL), the update of sasb200_adam_sched */
+/* Adam for all n (<= 16) parameter tensors in one launch, lr and bias
+ * corrections from sched (sasb200_lr_schedule): host arrays of n entries
+ * (device pointers; w[k], wt[k] may be NULL), each tensor updated as by
+ * sasb200_adam */
 int32_t sasb200_adam_multi(int32_t n, const int32_t *sizes, const int32_t *splits,
                            const float *const *grads, float *const *p, float *const *m,
                            float *const *v, void *const *w, void *const *wt, const int32_t *rows,

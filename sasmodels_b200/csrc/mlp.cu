@@ -19,7 +19,7 @@
 //                  way (A = dZ in smem, B = W_l^T streamed).
 //   gemm_nt        C_split = A[M x K] B[N x K]^T over a K range (split-K):
 //                  weight gradients dW = dZ^T H with the batch as K.
-//   + transpose, row sums/dots, loss gradient, Adam, feature packing.
+//   + transpose, column sums, loss gradient, Adam, feature packing.
 //
 // All launches return an error code; device-side waits are bounded and
 // report through *err (0 = ok).
@@ -441,20 +441,6 @@ __global__ void transpose_bf16(int rows, int cols, const __nv_bfloat16 *__restri
 }
 
 // out[r] = sum_c M[r][c] * (v ? v[c] : 1), one warp per row, fixed order
-__global__ void row_dot(int rows, int cols, const __nv_bfloat16 *__restrict__ M,
-                        const float *__restrict__ v, float *__restrict__ out)
-{
-    const int r = blockIdx.x*(blockDim.x/32) + threadIdx.x/32;
-    const int lane = threadIdx.x & 31;
-    if (r >= rows) return;
-    float s = 0.0f;
-    for (int c = lane; c < cols; c += 32)
-        s = fmaf(__bfloat162float(M[(size_t)r*cols + c]), v ? v[c] : 1.0f, s);
-    #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-    if (lane == 0) out[r] = s;
-}
-
 // Column sums of a row-major [rows x cols] bf16 matrix, each row weighted
 // by v[row] when v is given (the bias gradients from the dZ planes, the
 // output-layer gradient from the last h plane with v = dout).  Pass 1: one
@@ -552,27 +538,20 @@ __device__ __forceinline__ void adam_element(int i, int size, int splits,
     }
 }
 
-// sched (optional, device): {lr, bc1, bc2} of this step, written by
-// lr_schedule; replaces the by-value lr, bc1, bc2 (a CUDA graph of a
-// training step then replays with the schedule advancing on the device).
 __global__ void adam_step(int size, int splits, const float *__restrict__ grad, float *__restrict__ p,
                           float *__restrict__ m, float *__restrict__ v, float lr, float b1,
                           float b2, float eps, float bc1, float bc2, __nv_bfloat16 *__restrict__ w,
-                          __nv_bfloat16 *__restrict__ wt, int rows, int cols,
-                          const float *__restrict__ sched)
+                          __nv_bfloat16 *__restrict__ wt, int rows, int cols)
 {
     const int i = blockIdx.x*blockDim.x + threadIdx.x;
     if (i >= size) return;
-    if (sched) {
-        lr = sched[0];
-        bc1 = sched[1];
-        bc2 = sched[2];
-    }
     adam_element(i, size, splits, grad, p, m, v, lr, b1, b2, eps, bc1, bc2, w, wt, rows, cols);
 }
 
 // Every parameter tensor of the network in one launch (blockIdx.y = tensor),
-// the update of adam_step with lr and the bias corrections from sched.
+// the update of adam_step with lr and the bias corrections read from the
+// device (sched = {lr, bc1, bc2}, written by lr_schedule on the same stream,
+// so a CUDA graph of a training step replays with the schedule advancing).
 constexpr int ADAM_MAX_TENSORS = 16;
 struct AdamTensors {
     int n;
@@ -1659,16 +1638,6 @@ int32_t sasb200_transpose_bf16(int32_t rows, int32_t cols, const void *src, void
     return status("transpose_bf16");
 }
 
-int32_t sasb200_row_dot(int32_t rows, int32_t cols, const void *M, const float *v, float *out,
-                        void *stream)
-{
-    if (rows < 0 || cols < 0 || !M || !out) return -1;
-    if (!rows) return 0;
-    row_dot<<<(rows + 7)/8, 256, 0, (cudaStream_t)stream>>>(
-        rows, cols, static_cast<const __nv_bfloat16 *>(M), v, out);
-    return status("row_dot");
-}
-
 int32_t sasb200_loss_grad(int32_t n, int32_t n_pad, const float *out, const float *y, float delta,
                           float *dout, float *loss, void *stream)
 {
@@ -1688,21 +1657,7 @@ int32_t sasb200_adam(int32_t size, int32_t splits, const float *grad, float *p, 
     const float bc1 = 1.0f - powf(b1, (float)step), bc2 = 1.0f - powf(b2, (float)step);
     adam_step<<<(size + 255)/256, 256, 0, (cudaStream_t)stream>>>(
         size, splits, grad, p, m, v, lr, b1, b2, eps, bc1, bc2,
-        static_cast<__nv_bfloat16 *>(w), static_cast<__nv_bfloat16 *>(wt), rows, cols, nullptr);
-    return status("adam_step");
-}
-
-// Adam with lr and bias corrections read from the device (sched = {lr, bc1,
-// bc2}, written by sasb200_lr_schedule on the same stream).
-int32_t sasb200_adam_sched(int32_t size, int32_t splits, const float *grad, float *p, float *m,
-                           float *v, const float *sched, float b1, float b2, float eps, void *w,
-                           void *wt, int32_t rows, int32_t cols, void *stream)
-{
-    if (size <= 0 || splits <= 0 || !grad || !p || !m || !v || !sched) return -1;
-    if (wt && rows*cols != size) return -1;
-    adam_step<<<(size + 255)/256, 256, 0, (cudaStream_t)stream>>>(
-        size, splits, grad, p, m, v, 0.0f, b1, b2, eps, 1.0f, 1.0f,
-        static_cast<__nv_bfloat16 *>(w), static_cast<__nv_bfloat16 *>(wt), rows, cols, sched);
+        static_cast<__nv_bfloat16 *>(w), static_cast<__nv_bfloat16 *>(wt), rows, cols);
     return status("adam_step");
 }
 

@@ -55,10 +55,8 @@ def _lib():
     lib.sasb200_mlp_backward.argtypes = [I, I, P, P, P, P, P, P, P]
     lib.sasb200_gemm_nt.argtypes = [I, I, I, I, I, P, P, I, P, P, P]
     lib.sasb200_transpose_bf16.argtypes = [I, I, P, P, P]
-    lib.sasb200_row_dot.argtypes = [I, I, P, P, P, P]
     lib.sasb200_loss_grad.argtypes = [I, I, P, P, F, P, P, P]
     lib.sasb200_adam.argtypes = [I, I, P, P, P, P, F, F, F, F, I, P, P, I, I, P]
-    lib.sasb200_adam_sched.argtypes = [I, I, P, P, P, P, P, F, F, F, P, P, I, I, P]
     lib.sasb200_lr_schedule.argtypes = [P, P, I, I, F, F, F, P]
     lib.sasb200_adam_multi.argtypes = [I, P, P, P, P, P, P, P, P, P, P, P, F, F, F, P]
     lib.sasb200_col_sums.argtypes = [I, I, P, P, P, P, P]
@@ -70,11 +68,11 @@ def _lib():
     lib.sasb200_mlp_pack_t.argtypes = [P, P, P, P, P]
     lib.sasb200_mlp_backward_p.argtypes = [I, I, P, P, P, P, P, P, I, P]
     for name in ("sasb200_mlp_forward", "sasb200_mlp_backward", "sasb200_gemm_nt",
-                 "sasb200_transpose_bf16", "sasb200_row_dot", "sasb200_loss_grad",
+                 "sasb200_transpose_bf16", "sasb200_loss_grad",
                  "sasb200_adam", "sasb200_mlp_features", "sasb200_mlp_pack",
                  "sasb200_mlp_infer", "sasb200_mlp_serve", "sasb200_mlp_image_bytes",
                  "sasb200_mlp_pack_t", "sasb200_mlp_image_t_bytes", "sasb200_mlp_backward_p",
-                 "sasb200_adam_sched", "sasb200_lr_schedule", "sasb200_adam_multi",
+                 "sasb200_lr_schedule", "sasb200_adam_multi",
                  "sasb200_col_sums", "sasb200_col_sum_parts"):
         getattr(lib, name).restype = I
     lib.sasb200_mlp_last_error.restype = ct.c_char_p
