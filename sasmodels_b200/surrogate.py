@@ -94,6 +94,7 @@ class MLP:
             self.device = torch.device("cuda", torch.cuda.current_device())
         self.lib = _lib()
         self.stream = stream if stream is not None else torch.cuda.Stream(self.device)
+        self._side = [torch.cuda.Stream(self.device) for _ in range(4)]
         rng = np.random.default_rng(seed)
         shapes = [(HID, NIN), (HID, HID), (HID, HID), (HID, HID)]
         f32 = dict(dtype=torch.float32, device=self.device)
@@ -149,12 +150,15 @@ class MLP:
         self.z_save = torch.empty(4*n_pad*HID, **bf)
         self.h_save = torch.empty(4*n_pad*HID, **bf)
         self.dz_save = torch.empty(4*n_pad*HID, **bf)
-        self.t_a = torch.empty(HID*n_pad, **bf)        # transposed dZ
-        self.t_b = torch.empty(HID*n_pad, **bf)        # transposed h / x
+        # per layer (the four weight-gradient chains run concurrently):
+        # transposed dZ, transposed h / x, column-sum partials
+        self.t_a = [torch.empty(HID*n_pad, **bf) for _ in range(4)]
+        self.t_b = [torch.empty(HID*n_pad, **bf) for _ in range(4)]
         self.out = torch.empty(n_pad, **f32)
         self.dout = torch.empty(n_pad, **f32)
         self.sq = torch.empty(n_pad, **f32)
-        self.cs_part = torch.empty(self.lib.sasb200_col_sum_parts(n_pad)*HID, **f32)
+        parts = self.lib.sasb200_col_sum_parts(n_pad)*HID
+        self.cs_part = [torch.empty(parts, **f32) for _ in range(5)]
         self.splits = 32     # split-K of the weight gradients: 64+ CTAs at batch 8192
         self.gW = [torch.empty(self.splits*HID*(NIN if l == 0 else HID), **f32)
                    for l in range(4)]
@@ -251,31 +255,47 @@ class MLP:
                                                self.w_out.data_ptr(), self.dout.data_ptr(),
                                                self.z_save.data_ptr(), self.dz_save.data_ptr(),
                                                self.err.data_ptr(), 0, st), "backward")
+        # the weight-gradient chain of each layer (transposes, split-K GEMM,
+        # bias column sums) depends only on the planes: the four chains run on
+        # side streams forked from self.stream and joined before it goes on,
+        # so together they fill the SMs that one chain leaves idle
         plane = n_pad*HID
+        fork = torch.cuda.Event()
+        fork.record(self.stream)
+        joins = []
         for l in range(4):
+            side = self._side[l]
+            side.wait_event(fork)
+            ss = side.cuda_stream
             nb = NIN if l == 0 else HID
             dz = self.dz_save[l*plane:(l + 1)*plane]
-            self._check(lib.sasb200_transpose_bf16(n_pad, HID, dz.data_ptr(),
-                                                   self.t_a.data_ptr(), st), "transpose")
+            t_a, t_b = self.t_a[l], self.t_b[l]
+            self._check(lib.sasb200_transpose_bf16(n_pad, HID, dz.data_ptr(), t_a.data_ptr(), ss),
+                        "transpose")
             if l == 0:
                 src, cols = x, NIN
             else:
                 src, cols = self.h_save[(l - 1)*plane:l*plane], HID
-            self._check(lib.sasb200_transpose_bf16(n_pad, cols, src.data_ptr(),
-                                                   self.t_b.data_ptr(), st), "transpose")
-            self._check(lib.sasb200_gemm_nt(HID, nb, n_pad, n_pad, n_pad, self.t_a.data_ptr(),
-                                            self.t_b.data_ptr(), self.splits,
-                                            self.gW[l].data_ptr(), self.err.data_ptr(), st),
+            self._check(lib.sasb200_transpose_bf16(n_pad, cols, src.data_ptr(), t_b.data_ptr(), ss),
+                        "transpose")
+            self._check(lib.sasb200_gemm_nt(HID, nb, n_pad, n_pad, n_pad, t_a.data_ptr(),
+                                            t_b.data_ptr(), self.splits,
+                                            self.gW[l].data_ptr(), self.err.data_ptr(), ss),
                         "gemm_nt")
             # bias gradient: column sums of the dZ plane (zero on padding rows)
             self._check(lib.sasb200_col_sums(n_pad, HID, dz.data_ptr(), None,
-                                             self.cs_part.data_ptr(), self.gb[l].data_ptr(), st),
+                                             self.cs_part[l].data_ptr(), self.gb[l].data_ptr(), ss),
                         "col_sums")
+            done = torch.cuda.Event()
+            done.record(side)
+            joins.append(done)
         # output weights: columns of the last h plane weighted by dout
         h3 = self.h_save[3*plane:4*plane]
         self._check(lib.sasb200_col_sums(n_pad, HID, h3.data_ptr(), self.dout.data_ptr(),
-                                         self.cs_part.data_ptr(), self.gw.data_ptr(), st),
+                                         self.cs_part[4].data_ptr(), self.gw.data_ptr(), st),
                     "col_sums")
+        for done in joins:
+            self.stream.wait_event(done)
         with torch.cuda.stream(self.stream):
             self.gbo.copy_(self.dout[:n_pad].sum().reshape(1))
             loss = self.sq[:n].mean()
