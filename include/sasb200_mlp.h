@@ -45,15 +45,16 @@ int32_t sasb200_mlp_infer(int32_t n, int32_t n_pad, const void *x, const void *x
                           const float *b_out, float *out, void *z_save, void *h_save,
                           int32_t *err, int32_t blocks, void *stream);
 
-/* inference only, same image and arguments without the z/h planes: the
- * overlapped kernel (a dedicated MMA warp, two TMEM accumulators, layer
- * l+1's MMAs running under layer l's epilogue chunk by chunk).  Hidden
- * activations bitwise those of sasb200_mlp_infer; out differs only by the
- * order of the output dot's sums. */
+/* the same forward through the overlapped kernel (a dedicated MMA warp, two
+ * TMEM accumulators, layer l+1's MMAs running under layer l's epilogue chunk
+ * by chunk), same image and arguments.  Hidden activations and the z/h
+ * planes bitwise those of sasb200_mlp_infer; out differs only by the order
+ * of the output dot's sums.  Used for inference (planes NULL) and for the
+ * training forward. */
 int32_t sasb200_mlp_serve(int32_t n, int32_t n_pad, const void *x, const void *x_lo,
                           const void *img, const float *const *b, const float *w_out,
-                          const float *b_out, float *out, int32_t *err, int32_t blocks,
-                          void *stream);
+                          const float *b_out, float *out, void *z_save, void *h_save,
+                          int32_t *err, int32_t blocks, void *stream);
 
 /* pipelined backward (training): W3^T, W2^T, W1^T packed once per weight
  * update by sasb200_mlp_pack_t into sasb200_mlp_image_t_bytes() bytes; dZ

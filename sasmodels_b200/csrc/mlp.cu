@@ -909,8 +909,8 @@ mlp_infer(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
 }
 
 // ------------------------------------------------------------------ serve --
-// mlp_serve: inference only (no z/h planes), with the tensor core and the
-// epilogue busy at the same time.  Arithmetic per element as mlp_infer
+// mlp_serve: the forward pass (inference, or training with the z/h planes)
+// with the tensor core and the epilogue busy at the same time.  Arithmetic per element as mlp_infer
 // (bias, SiLU, the compensated hi/lo split rounded to nearest), so the
 // hidden activations are bitwise those of mlp_infer; the output dot sums
 // the 256 columns in another order (four partial sums per row).
@@ -966,13 +966,28 @@ __device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity)
 }
 
 // z = acc + bias and h = silu(z) for 8 columns.
-__device__ __forceinline__ void sv_silu8(const uint32_t (&a)[8], const float *bias, float (&h)[8])
+__device__ __forceinline__ void sv_silu8(const uint32_t (&a)[8], const float *bias, float (&z)[8],
+                                         float (&h)[8])
 {
     const float4 b0 = *reinterpret_cast<const float4 *>(bias);
     const float4 b1 = *reinterpret_cast<const float4 *>(bias + 4);
     const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
     #pragma unroll
-    for (int j = 0; j < 8; ++j) h[j] = silu(__uint_as_float(a[j]) + bb[j]);
+    for (int j = 0; j < 8; ++j) {
+        z[j] = __uint_as_float(a[j]) + bb[j];
+        h[j] = silu(z[j]);
+    }
+}
+
+// 8 floats as bf16 (round to nearest) in one 16-byte store
+__device__ __forceinline__ void save8(__nv_bfloat16 *dst, const float (&v)[8])
+{
+    uint4 u;
+    u.x = pack2(v[0], v[1]);
+    u.y = pack2(v[2], v[3]);
+    u.z = pack2(v[4], v[5]);
+    u.w = pack2(v[6], v[7]);
+    *reinterpret_cast<uint4 *>(dst) = u;
 }
 
 template <int RND>
@@ -1152,6 +1167,7 @@ mlp_serve(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
         const int quad = warp & 3, slot = warp >> 2;
         const int row = 32*quad + lane;
         const int cs = SV_COLS*slot;
+        const size_t plane = (size_t)n_tiles*TM*HID;
         const uint32_t lane_base = (uint32_t)(32*quad) << 16;
         bool ok = true;
         for (int k = 0; k < my_tiles && ok; ++k) {
@@ -1189,8 +1205,14 @@ mlp_serve(int n, int n_tiles, const __nv_bfloat16 *__restrict__ x,
                     #pragma unroll
                     for (int r = 0; r < RND; ++r) {
                         const int c = RND*j + r;
-                        float h[8];
-                        sv_silu8(ra[r], bias + KCI*c, h);
+                        float z[8], h[8];
+                        sv_silu8(ra[r], bias + KCI*c, z, h);
+                        if (prm.z_save != nullptr) {   // training: the planes of every layer
+                            const size_t at = (size_t)l*plane + (size_t)(row0 + row)*HID
+                                            + KCI*c + cs;
+                            save8(prm.z_save + at, z);
+                            save8(prm.h_save + at, h);
+                        }
                         if (l < 3) {
                             uint4 hi, lo;
                             uint32_t *hp = &hi.x, *lp = &lo.x;
@@ -1513,14 +1535,16 @@ int32_t sasb200_mlp_infer(int32_t n, int32_t n_pad, const void *x, const void *x
     return status("mlp_infer");
 }
 
-// Inference only: out[n] for x, x_lo [n_pad x 16] with the packed weights,
-// through the overlapped kernel (mlp_serve); persistent grid of at most
-// `blocks` CTAs (0 = one per SM).  err receives 1, 2 or 3 if a pipeline
+// out[n] for x, x_lo [n_pad x 16] with the packed weights through the
+// overlapped kernel (mlp_serve), and, when z_save/h_save are given, the
+// pre-activations and activations of all four layers ([4][n_pad x 256] bf16
+// each, those of mlp_infer) for training; persistent grid of at most
+// `blocks` CTAs (0 = one per SM).  err receives 1, 2, 3 or 4 if a pipeline
 // wait ran out.
 int32_t sasb200_mlp_serve(int32_t n, int32_t n_pad, const void *x, const void *x_lo,
                           const void *img, const float *const *b, const float *w_out,
-                          const float *b_out, float *out, int32_t *err, int32_t blocks,
-                          void *stream)
+                          const float *b_out, float *out, void *z_save, void *h_save,
+                          int32_t *err, int32_t blocks, void *stream)
 {
     errbuf()[0] = 0;
     if (n < 0 || n_pad % TM || n > n_pad || !x || !x_lo || !img || !b || !w_out || !b_out
@@ -1537,8 +1561,10 @@ int32_t sasb200_mlp_serve(int32_t n, int32_t n_pad, const void *x, const void *x
     for (int l = 0; l < 4; ++l) prm.b[l] = b[l];
     prm.w_out = w_out;
     prm.b_out = b_out;
-    prm.z_save = nullptr;
-    prm.h_save = nullptr;
+    if ((z_save == nullptr) != (h_save == nullptr))
+        return (std::snprintf(errbuf(), 256, "z_save and h_save go together"), -1);
+    prm.z_save = static_cast<__nv_bfloat16 *>(z_save);
+    prm.h_save = static_cast<__nv_bfloat16 *>(h_save);
     const int n_tiles = n_pad/TM;
     if (blocks == 0) {
         int dev = 0, sms = 0;

@@ -64,7 +64,7 @@ def _lib():
     lib.sasb200_mlp_features.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P]
     lib.sasb200_mlp_pack.argtypes = [P, P, P, P, P, P]
     lib.sasb200_mlp_infer.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P, I, P]
-    lib.sasb200_mlp_serve.argtypes = [I, I, P, P, P, P, P, P, P, P, I, P]
+    lib.sasb200_mlp_serve.argtypes = [I, I, P, P, P, P, P, P, P, P, P, P, I, P]
     lib.sasb200_mlp_pack_t.argtypes = [P, P, P, P, P]
     lib.sasb200_mlp_backward_p.argtypes = [I, I, P, P, P, P, P, P, I, P]
     for name in ("sasb200_mlp_forward", "sasb200_mlp_backward", "sasb200_gemm_nt",
@@ -210,7 +210,7 @@ class MLP:
         self._pack()
         self._check(self.lib.sasb200_mlp_serve(
             n, n_pad, x.data_ptr(), x_lo.data_ptr(), self.img.data_ptr(), self._ptrs(self.b),
-            self.w_out.data_ptr(), self.b_out.data_ptr(), self._infer_out.data_ptr(),
+            self.w_out.data_ptr(), self.b_out.data_ptr(), self._infer_out.data_ptr(), None, None,
             self.err.data_ptr(), int(blocks), self.stream.cuda_stream), "mlp_serve")
         return self._infer_out[:n_pad]
 
@@ -241,9 +241,10 @@ class MLP:
         n_pad = x.shape[0]
         st = self.stream.cuda_stream
         lib = self.lib
-        # forward with the z/h planes and backward through the pipelined
-        # persistent kernels (weights streamed from the packed images)
-        self._check(lib.sasb200_mlp_infer(
+        # forward with the z/h planes through the overlapped kernel, backward
+        # through the pipelined persistent kernel (weights streamed from the
+        # packed images)
+        self._check(lib.sasb200_mlp_serve(
             n, n_pad, x.data_ptr(), x_lo.data_ptr(), self.img.data_ptr(), self._ptrs(self.b),
             self.w_out.data_ptr(), self.b_out.data_ptr(), self.out.data_ptr(),
             self.z_save.data_ptr(), self.h_save.data_ptr(), self.err.data_ptr(), 0, st),

@@ -255,9 +255,10 @@ def test_tc_infer_tracks_training(cuda):
 
 @pytest.mark.gpu
 def test_tc_pipelined_training_kernels_match(cuda):
-    """The pipelined forward (with z/h planes) and backward give the planes
-    of the one-CTA-per-tile training kernels bit for bit (same MMAs in the
-    same order, same epilogue arithmetic)."""
+    """The pipelined forward (with z/h planes), the overlapped forward that
+    training uses, and the pipelined backward give the planes of the
+    one-CTA-per-tile training kernels bit for bit (same MMAs in the same
+    order, same epilogue arithmetic)."""
     import ctypes as ct
     import torch
     from sasmodels_b200.surrogate import HID, pad128
@@ -293,6 +294,18 @@ def test_tc_pipelined_training_kernels_match(cuda):
     assert net.errors() == 0
     assert torch.equal(z1, z2) and torch.equal(h1, h2)
     assert torch.equal(d1, d2)
+    # the overlapped kernel writes the same planes (the training forward);
+    # several tiles per CTA so its barrier phases wrap
+    z3, h3 = torch.zeros_like(z1), torch.zeros_like(h1)
+    o3 = torch.zeros_like(o1)
+    net._check(lib.sasb200_mlp_serve(n, n_pad, x.data_ptr(), xlo.data_ptr(), net.img.data_ptr(),
+                                     net._ptrs(net.b), net.w_out.data_ptr(),
+                                     net.b_out.data_ptr(), o3.data_ptr(), z3.data_ptr(),
+                                     h3.data_ptr(), net.err.data_ptr(), 5, st), "serve")
+    net.stream.synchronize()
+    assert net.errors() == 0
+    assert torch.equal(z1, z3) and torch.equal(h1, h3)
+    torch.testing.assert_close(o3[:n], o1[:n], rtol=1e-5, atol=1e-6*float(o1[:n].abs().max()))
 
 
 @pytest.mark.gpu
