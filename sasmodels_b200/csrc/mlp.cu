@@ -17,9 +17,19 @@
 //   mlp_backward   dZ3 = dout w_out * silu'(z3), then dZ(l-1) = (dZl W_l) *
 //                  silu'(z(l-1)) through the three 256x256 layers, the same
 //                  way (A = dZ in smem, B = W_l^T streamed).
+//   mlp_infer,     persistent pipelined forms of the two (weights bulk-copied
+//   mlp_backward_p through a shared-memory ring); they give the planes of
+//                  mlp_forward / mlp_backward bit for bit.
+//   mlp_serve      the forward with the tensor core and the epilogue working
+//                  at once (a dedicated MMA warp, two TMEM accumulators,
+//                  layer l+1's MMAs under layer l's epilogue chunk by chunk);
+//                  serves inference and, with the planes, the training
+//                  forward.
 //   gemm_nt        C_split = A[M x K] B[N x K]^T over a K range (split-K):
 //                  weight gradients dW = dZ^T H with the batch as K.
-//   + transpose, column sums, loss gradient, Adam, feature packing.
+//   + transpose, column sums (bias gradients), loss gradient, the learning
+//     rate schedule, Adam (one tensor, or every tensor in one launch),
+//     feature packing.
 //
 // All launches return an error code; device-side waits are bounded and
 // report through *err (0 = ok).
