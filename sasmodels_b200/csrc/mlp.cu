@@ -72,9 +72,14 @@ __device__ __forceinline__ float silu(float z)
     return fmaf(hz, t, hz);
 }
 
+// silu'(z) = s (1 + z (1 - s)) with the sigmoid s = (1 + tanh(z/2))/2 taken
+// as in silu above, so the backward pass differentiates the function the
+// forward pass evaluates (one MUFU operation instead of an exp and a divide).
 __device__ __forceinline__ float dsilu(float z)
 {
-    const float s = 1.0f/(1.0f + __expf(-z));
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f*z));
+    const float s = fmaf(0.5f, t, 0.5f);
     return s*(1.0f + z*(1.0f - s));
 }
 
