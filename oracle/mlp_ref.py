@@ -7,9 +7,9 @@ SiLU, z = h W^T + b, out = h3 . w_out + b_out, MSE loss.  With
 ``emulate_bf16=True`` every value the GPU stores as BF16 (weights, saved
 z/h, dZ; inputs and hidden activations as a compensated hi + lo BF16 pair) is
 rounded the same way, so the device gradients can be compared tightly; with ``False`` it is
-the plain FP64 mathematics the kernels approximate.  SiLU here is exact; the kernels evaluate
-it as z/2 + (z/2) tanh(z/2) with the hardware tanh approximation (relative error about
-2^-11), which the tests' tolerances cover.
+the plain FP64 mathematics the kernels approximate.  SiLU and its derivative here are exact;
+the kernels take the sigmoid in both as (1 + tanh(z/2))/2 with the hardware tanh
+approximation (relative error about 2^-11), which the tests' tolerances cover.
 """
 
 import numpy as np
